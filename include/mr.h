@@ -1,0 +1,232 @@
+/*
+ * mr.h — C-ABI of the B200-native reordered-SpMV library (libmr.so).
+ *
+ * Drop-in boundary for the reordered-SpMV path of Zhangq388/MATRIX-REORDER.
+ * Each entry point names the reference interface it replaces as
+ * `file:line` in that project. The reference has no FFI layer of its own; its
+ * operator API is the C++ template struct GRAPH<V> (include/class.cuh:58-97)
+ * and the TILE / merbit_kernel templates (include/merbit.cuh). These entry
+ * points are what a binding of that API binds.
+ *
+ * Conventions
+ *  - Every call returns an mr_status (0 = MR_OK); no C++ exception crosses
+ *    the ABI. mr_status_string() gives a message.
+ *  - Matrices are textbook CSR: row i holds colidx[rowptr[i] .. rowptr[i+1]).
+ *    (The reference stores the transpose: its `col_ind` is our row and its
+ *    `row_ind` our column, src/class.cu:1342, :1372.)
+ *  - Pointers named *_dev are device memory, *_host host memory. Matrix and
+ *    vector buffers are owned by the caller; plan objects own their
+ *    descriptors. Work is enqueued on `stream` (a cudaStream_t, NULL = the
+ *    legacy default stream) and is ordered on it. Calls on different streams
+ *    may run concurrently.
+ *  - 32-bit indices: n_rows, n_cols and nnz must be < 2^31.
+ */
+#ifndef MR_H
+#define MR_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mr_status {
+    MR_OK = 0,
+    MR_ERR_INVALID_ARG = 1,   /* bad size, null pointer or option */
+    MR_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    MR_ERR_NOMEM = 3,         /* device or host allocation failed */
+    MR_ERR_INVALID_PERM = 4,  /* permutation is not a bijection of [0, n) */
+    MR_ERR_UNSUPPORTED = 5,   /* dtype / option not supported by this entry */
+    MR_ERR_TIMEOUT = 6,       /* a bounded wait expired */
+    MR_ERR_BUSY = 7,          /* admission refused: no slot / no memory */
+    MR_ERR_NOT_FOUND = 8,     /* unknown id */
+    MR_ERR_INTERNAL = 9,      /* a device-side consistency check failed */
+    MR_ERR_PREDICT = 10       /* predictor produced a non-finite or <= 0 value */
+} mr_status;
+
+typedef enum mr_dtype {
+    MR_F32 = 0,
+    MR_F16 = 1,
+    MR_BF16 = 2
+} mr_dtype;
+
+/* A CSR matrix in device memory (values of `dtype`). */
+typedef struct mr_csr_view {
+    int32_t n_rows;
+    int32_t n_cols;
+    int64_t nnz;
+    const int32_t* rowptr; /* n_rows + 1 */
+    const int32_t* colidx; /* nnz, sorted within each row for MERBIT/RD */
+    const void* vals;      /* nnz */
+    int32_t dtype;         /* mr_dtype */
+} mr_csr_view;
+
+const char* mr_status_string(int status);
+int mr_version(void);
+/* Last CUDA error text seen by this thread (empty if none). */
+const char* mr_last_error(void);
+
+/* *valid_host = 1 if rowptr[0] == 0, rowptr is non-decreasing,
+ * rowptr[n_rows] == nnz and every column index is in [0, n_cols).
+ * The SpMV entry points do not re-check this on every call; plan creation
+ * and mr_permute_csr do. Synchronises `stream`. No reference counterpart
+ * (the reference performs no input validation). */
+int mr_csr_validate(const mr_csr_view* A, int* valid_host, void* stream);
+
+/* ------------------------------------------------------------- SpMV ---- */
+
+/* y = A x, FP32 x/y, values of A->dtype, FP32 accumulation. Plain CSR path.
+ * Replaces the cusparseSpMV(CSR_ALG1) loop of GRAPH::spmv(env, "csr")
+ * (src/class.cu:1359-1397). */
+int mr_spmv_csr(const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
+
+/* MERBIT merge-path plan. The descriptor arrays are bit-identical to those
+ * TILE<BLOCK,SIGMA>::TILE builds (include/merbit.cuh:134-155, Tile_Kernel
+ * :55-131): tile_x/tile_y[tile_num+1] (bit 31 of tile_y = single-row tile)
+ * and lane_desc[lane_num] (32-bit words for sigma < 15, 64-bit otherwise).
+ * sigma: merge items per lane, 1..42 (reference 14). block: threads per CTA
+ * of the SpMV kernel, a multiple of 32 in [32, 1024] (reference 256); 0
+ * picks the default. The plan also owns the per-tile carry-out scratch.
+ * The rowptr of A must stay unchanged while the plan is used. */
+typedef struct mr_merbit_plan mr_merbit_plan;
+
+typedef struct mr_merbit_plan_info {
+    int32_t sigma;
+    int32_t block;
+    int32_t n_rows;
+    int64_t nnz;
+    int32_t lane_num;
+    int32_t tile_num;
+    int32_t desc_bytes;           /* 4 or 8 */
+    const uint32_t* tile_x_dev;   /* tile_num + 1 */
+    const uint32_t* tile_y_dev;   /* tile_num + 1 */
+    const void* lane_desc_dev;    /* lane_num words of desc_bytes */
+} mr_merbit_plan_info;
+
+int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stream, mr_merbit_plan** plan);
+/* Replaces TILE::~TILE (include/merbit.cuh:256-263). Synchronises the device
+ * before freeing. */
+int mr_merbit_plan_destroy(mr_merbit_plan* plan);
+int mr_merbit_plan_get_info(const mr_merbit_plan* plan, mr_merbit_plan_info* info);
+
+/* y = A x with the MERBIT plan. Replaces the merbit_kernel<V,256,14> launch
+ * loop of GRAPH::spmv(env, "merbit") (src/class.cu:1407-1430,
+ * include/merbit.cuh:408-493). Deterministic: rows spanning tiles are
+ * finished by an FP64 carry fix-up instead of float atomics, so no second
+ * output buffer (the reference's d_z) is needed. */
+int mr_spmv_merbit(const mr_merbit_plan* plan, const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
+
+/* ------------------------------------------------------ permutation ---- */
+
+/* B = P A P^T: B[perm[r], perm[c]] = A[r, c], columns sorted within rows,
+ * equal columns kept in source order. Output arrays are caller-allocated
+ * (n_rows+1, nnz, nnz of A->dtype); the matrix must be square.
+ * Replaces the perm scatter + gather relabel + GRAPH::sort(false) + coo2csr
+ * of GRAPH::gorder4 (src/class.cu:2686-2705, :423-457, :1342).
+ * Synchronises `stream` and returns MR_ERR_INVALID_PERM if perm is not a
+ * bijection (output then undefined). */
+int mr_permute_csr(const mr_csr_view* A, const int32_t* perm_old2new_dev,
+                   int32_t* out_rowptr_dev, int32_t* out_colidx_dev, void* out_vals_dev, void* stream);
+
+/* out[perm[i]] = in[i] when inverse == 0 (x' = P x), out[i] = in[perm[i]]
+ * when inverse != 0 (y = P^T y', the check gather of src/class.cu:1437-1440). */
+int mr_permute_vector(int32_t n, const int32_t* perm_old2new_dev, const float* in_dev, float* out_dev,
+                      int inverse, void* stream);
+
+/* perm_new2old[perm_old2new[i]] = i (the scatter of src/class.cu:2688-2689). */
+int mr_perm_invert(int32_t n, const int32_t* perm_dev, int32_t* inv_dev, void* stream);
+
+/* *valid_host = 1 if perm is a bijection of [0, n). Replaces check_perm
+ * (include/utils.cuh:5-55), which only prints. Synchronises `stream`. */
+int mr_check_perm(const int32_t* perm_dev, int32_t n, int* valid_host, void* stream);
+
+/* ------------------------------------------- reuse-distance features ---- */
+
+/* Exact sector reuse-distance histogram of the x-access stream (colidx in
+ * CSR order): sector = col / sector_size; for each reuse, RD = number of
+ * distinct sectors touched since the previous use; counts[b] for
+ * b = upper_bound(edges, RD). counts_host has nedges+1 entries; *valid_host
+ * gets the number of reuses. Counts are exact (integers). Replaces
+ * compute_sector_rd_histogram (src/class.cu:892-936), whose probabilities are
+ * counts[b] / valid. Synchronises `stream`. */
+int mr_rd_hist_exact(const int32_t* stream_dev, int64_t nnz, int32_t ncols, int32_t sector_size,
+                     const int32_t* edges_host, int32_t nedges, int64_t* counts_host, int64_t* valid_host,
+                     void* stream);
+
+/* Sampled reuse distance with HyperLogLog registers, same samples, statuses
+ * and estimates as sampled_hll_rd_block_gpu (src/class.cu:1133-1261):
+ * status 0 = found (binned by estimate), 1 = cold, 2 = estimate above
+ * rd_cap (last bin), 3 = max_scan reached. hll_p <= 0 means 12; it is
+ * clamped to [4, 14]. stats_host[4] = {found, cold, large, unresolved}.
+ * est/status/pos (device, `samples` entries each) are optional outputs.
+ * Synchronises `stream`. */
+int mr_rd_hist_sampled(const int32_t* stream_dev, int32_t nnz, int32_t samples, int32_t sector_size,
+                       int32_t rd_cap, int32_t hll_p, int32_t max_scan, uint32_t seed,
+                       const int32_t* edges_host, int32_t nedges, int64_t* counts_host, int64_t* stats_host,
+                       float* est_dev, int32_t* status_dev, int32_t* pos_dev, void* stream);
+
+/* Sample seed of sampled_hll_rd_block_gpu (src/class.cu:1203). */
+uint32_t mr_hll_seed(int32_t graph_id, int32_t stream_type);
+
+/* ----------------------------------------------------------- predictor ---- */
+
+typedef enum mr_model {
+    MR_MODEL_MERBIT_SAMPLED = 0, /* include/model.cuh, ridge/out/merbit/sampled */
+    MR_MODEL_MERBIT_EXACT = 1,   /* ridge/out/merbit/exact */
+    MR_MODEL_CSR_SAMPLED = 2,    /* ridge/out/csr/sampled */
+    MR_MODEL_CSR_EXACT = 3       /* ridge/out/csr/exact */
+} mr_model;
+
+/* exp(b + sum w_i r_i) over the 10 RD-bin probabilities. Replaces
+ * rd_merbit_model::PredictSpeedup (include/model.cuh:91-94); returns
+ * MR_ERR_PREDICT when the value is not finite or <= 0 (the reference throws,
+ * src/class.cu:1317-1320). */
+int mr_predict_speedup(int model, const double* features10, double* speedup);
+
+/* Sampled RD (reference settings: sector 32, 30960 samples, p = 12,
+ * max_scan 0, the 9 edges of src/class.cu:1267) + PredictSpeedup.
+ * Replaces GRAPH::locality_predict (src/class.cu:1263-1326). features10 may
+ * be NULL. */
+int mr_locality_predict(const int32_t* stream_dev, int32_t nnz, int32_t ncols, int32_t graph_id,
+                        double* features10, float* speedup, void* stream);
+
+/* ------------------------------------------------------------- pGOrder ---- */
+
+/* Partition size of gorder4: GRAPH::get_width (src/class.cu:733-750). */
+int32_t mr_pgorder_width(int32_t n_rows, int64_t nnz);
+
+/* pGOrder ordering on the host: perm_new2old[new] = old, bit-identical to
+ * GRAPH::gorder4's order_on_cpu tasks (src/class.cu:2608-2690, :2220-2314,
+ * include/integer_heap.cuh). A is a square host CSR with sorted columns.
+ * vsize <= 0 uses mr_pgorder_width; threads <= 0 uses all cores. */
+int mr_pgorder(int32_t n, const int32_t* rowptr_host, const int32_t* colidx_host, int32_t vsize,
+               int32_t width, int32_t threads, uint32_t* perm_new2old_host);
+
+/* ------------------------------------------ GRAPH-style host object ---- */
+
+/* A square matrix resident on the device with its current permutation
+ * (perm[old] = new), mirroring GRAPH<float> (include/class.cuh:58-97). */
+typedef struct mr_graph mr_graph;
+
+int mr_graph_create(int32_t n, int64_t nnz, const int32_t* rowptr_host, const int32_t* colidx_host,
+                    const void* vals_host, int32_t dtype, int32_t graph_id, mr_graph** g);
+int mr_graph_destroy(mr_graph* g);
+/* GRAPH::gorder4(env, vsize, width) (src/class.cu:2608-2722): host pGOrder,
+ * then the device relabel; ms_order/ms_relabel may be NULL. */
+int mr_graph_gorder4(mr_graph* g, int32_t vsize, int32_t width, double* ms_order, double* ms_relabel);
+/* GRAPH::locality_predict (src/class.cu:1263-1326) on the current order. */
+int mr_graph_locality_predict(mr_graph* g, double* features10, float* speedup);
+/* GRAPH::spmv(env, method) (src/class.cu:1331-1454): method "csr" or
+ * "merbit"; runs `iters` SpMVs with x = x_host (original numbering, NULL =
+ * all ones as the reference) and returns y in the original numbering.
+ * ms_plan/ms_spmv may be NULL (ms_spmv is per SpMV). */
+int mr_graph_spmv(mr_graph* g, const char* method, int32_t iters, const float* x_host, float* y_host,
+                  double* ms_plan, double* ms_spmv);
+/* Current permutation perm[old] = new, and the current device CSR view. */
+int mr_graph_get_perm(const mr_graph* g, int32_t* perm_host);
+int mr_graph_view(const mr_graph* g, mr_csr_view* view);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MR_H */

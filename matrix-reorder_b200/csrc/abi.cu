@@ -1,0 +1,211 @@
+// extern "C" entry points of libmr: argument checks, plan ownership and
+// dispatch to the kernels. Declared in include/mr.h.
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace mr {
+
+static thread_local std::string g_last_error;
+
+void note_cuda_error(cudaError_t e, const char* what, const char* file, int line)
+{
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%s: %s (%s:%d)", cudaGetErrorString(e), what, file, line);
+    g_last_error = buf;
+}
+
+void note_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+static int check_view(const mr_csr_view* A, bool need_square)
+{
+    if (!A) return MR_ERR_INVALID_ARG;
+    if (A->n_rows < 0 || A->n_cols < 0 || A->nnz < 0 || A->nnz > INT32_MAX) return MR_ERR_INVALID_ARG;
+    if (A->dtype != MR_F32 && A->dtype != MR_F16 && A->dtype != MR_BF16) return MR_ERR_UNSUPPORTED;
+    if (!A->rowptr) return MR_ERR_INVALID_ARG;
+    if (A->nnz > 0 && (!A->colidx || !A->vals)) return MR_ERR_INVALID_ARG;
+    if (need_square && A->n_rows != A->n_cols) return MR_ERR_INVALID_ARG;
+    return MR_OK;
+}
+
+}  // namespace mr
+
+using namespace mr;
+
+struct mr_merbit_plan {
+    MerbitPlan p;
+};
+
+extern "C" {
+
+const char* mr_status_string(int s)
+{
+    switch (s) {
+    case MR_OK: return "ok";
+    case MR_ERR_INVALID_ARG: return "invalid argument";
+    case MR_ERR_CUDA: return "CUDA error";
+    case MR_ERR_NOMEM: return "out of memory";
+    case MR_ERR_INVALID_PERM: return "permutation is not a bijection";
+    case MR_ERR_UNSUPPORTED: return "unsupported dtype or option";
+    case MR_ERR_TIMEOUT: return "bounded wait expired";
+    case MR_ERR_BUSY: return "admission refused";
+    case MR_ERR_NOT_FOUND: return "unknown id";
+    case MR_ERR_INTERNAL: return "internal consistency check failed";
+    case MR_ERR_PREDICT: return "predictor returned an invalid speedup";
+    default: return "unknown status";
+    }
+}
+
+int mr_version(void) { return 10000; }
+
+const char* mr_last_error(void) { return g_last_error.c_str(); }
+
+int mr_spmv_csr(const mr_csr_view* A, const float* x, float* y, void* stream)
+{
+    MR_TRY(check_view(A, false));
+    if (A->n_rows > 0 && (!y || (A->nnz > 0 && !x))) return MR_ERR_INVALID_ARG;
+    return launch_csr_spmv(A->n_rows, A->nnz, A->rowptr, A->colidx, A->vals, A->dtype, x, y, as_stream(stream));
+}
+
+int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stream, mr_merbit_plan** out)
+{
+    if (!out) return MR_ERR_INVALID_ARG;
+    *out = nullptr;
+    MR_TRY(check_view(A, false));
+    if (sigma == 0) sigma = 14;
+    if (block == 0) block = 256;
+    if (sigma < 1 || sigma > 42) return MR_ERR_INVALID_ARG;
+    if (block != 128 && block != 256 && block != 512) return MR_ERR_UNSUPPORTED;
+    const int64_t items = (int64_t)A->n_rows + A->nnz;
+    if (items + 32ll * sigma * 257 > (int64_t)INT32_MAX) return MR_ERR_INVALID_ARG;
+    {
+        int ok = 0;
+        MR_TRY(validate_csr(*A, &ok, as_stream(stream)));
+        if (!ok) return MR_ERR_INVALID_ARG;
+    }
+    auto* h = new (std::nothrow) mr_merbit_plan;
+    if (!h) return MR_ERR_NOMEM;
+    MerbitPlan& p = h->p;
+    p.sigma = sigma;
+    p.block = block;
+    p.n_rows = A->n_rows;
+    p.nnz = A->nnz;
+    p.lane_num = (int)((items + sigma - 1) / sigma);
+    p.tile_num = (p.lane_num + 31) / 32;
+    cudaGetDevice(&p.device);
+    const size_t desc_bytes = sigma < 15 ? 4 : 8;
+    cudaStream_t st = as_stream(stream);
+    auto fail = [&](int code) {
+        cudaFree(p.tile_x);
+        cudaFree(p.tile_y);
+        cudaFree(p.lane_desc);
+        cudaFree(p.carry);
+        delete h;
+        return code;
+    };
+    if (cudaMalloc(&p.tile_x, sizeof(uint32_t) * ((size_t)p.tile_num + 1)) != cudaSuccess ||
+        cudaMalloc(&p.tile_y, sizeof(uint32_t) * ((size_t)p.tile_num + 1)) != cudaSuccess ||
+        cudaMalloc(&p.lane_desc, desc_bytes * (size_t)std::max(p.lane_num, 1)) != cudaSuccess ||
+        cudaMalloc(&p.carry, sizeof(float) * (size_t)std::max(p.tile_num, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(MR_ERR_NOMEM);
+    }
+    int s = launch_merbit_plan(A->rowptr, A->n_rows, (int)A->nnz, sigma, p.lane_num, p.tile_num, p.tile_x, p.tile_y,
+                               p.lane_desc, st);
+    if (s != MR_OK) return fail(s);
+    *out = h;
+    return MR_OK;
+}
+
+int mr_merbit_plan_destroy(mr_merbit_plan* h)
+{
+    if (!h) return MR_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != h->p.device) cudaSetDevice(h->p.device);
+    cudaDeviceSynchronize();
+    cudaFree(h->p.tile_x);
+    cudaFree(h->p.tile_y);
+    cudaFree(h->p.lane_desc);
+    cudaFree(h->p.carry);
+    if (dev != h->p.device) cudaSetDevice(dev);
+    delete h;
+    return MR_OK;
+}
+
+int mr_merbit_plan_get_info(const mr_merbit_plan* h, mr_merbit_plan_info* info)
+{
+    if (!h || !info) return MR_ERR_INVALID_ARG;
+    const MerbitPlan& p = h->p;
+    info->sigma = p.sigma;
+    info->block = p.block;
+    info->n_rows = p.n_rows;
+    info->nnz = p.nnz;
+    info->lane_num = p.lane_num;
+    info->tile_num = p.tile_num;
+    info->desc_bytes = p.sigma < 15 ? 4 : 8;
+    info->tile_x_dev = p.tile_x;
+    info->tile_y_dev = p.tile_y;
+    info->lane_desc_dev = p.lane_desc;
+    return MR_OK;
+}
+
+int mr_spmv_merbit(const mr_merbit_plan* h, const mr_csr_view* A, const float* x, float* y, void* stream)
+{
+    if (!h) return MR_ERR_INVALID_ARG;
+    MR_TRY(check_view(A, false));
+    const MerbitPlan& p = h->p;
+    if (A->n_rows != p.n_rows || A->nnz != p.nnz) return MR_ERR_INVALID_ARG;
+    if (!merbit_sigma_supported(p.sigma)) return MR_ERR_UNSUPPORTED;
+    if (p.n_rows > 0 && (!y || (p.nnz > 0 && !x))) return MR_ERR_INVALID_ARG;
+    return launch_merbit_spmv(p, A->colidx, A->vals, A->dtype, x, y, p.carry, as_stream(stream));
+}
+
+int mr_permute_csr(const mr_csr_view* A, const int32_t* perm, int32_t* out_rowptr, int32_t* out_colidx,
+                   void* out_vals, void* stream)
+{
+    MR_TRY(check_view(A, true));
+    if (!perm && A->n_rows > 0) return MR_ERR_INVALID_ARG;
+    if (!out_rowptr || (A->nnz > 0 && (!out_colidx || !out_vals))) return MR_ERR_INVALID_ARG;
+    return permute_csr(*A, perm, out_rowptr, out_colidx, out_vals, as_stream(stream));
+}
+
+int mr_permute_vector(int32_t n, const int32_t* perm, const float* in, float* out, int inverse, void* stream)
+{
+    if (n < 0 || (n > 0 && (!perm || !in || !out))) return MR_ERR_INVALID_ARG;
+    return launch_permute_vector(n, perm, in, out, inverse, as_stream(stream));
+}
+
+int mr_perm_invert(int32_t n, const int32_t* perm, int32_t* inv, void* stream)
+{
+    if (n < 0 || (n > 0 && (!perm || !inv))) return MR_ERR_INVALID_ARG;
+    if (n == 0) return MR_OK;
+    cudaStream_t st = as_stream(stream);
+    DevBuf flag;
+    MR_TRY(flag.alloc(sizeof(int), st));
+    MR_CUDA_TRY(cudaMemsetAsync(flag.p, 0, sizeof(int), st));
+    MR_TRY(launch_perm_invert(n, perm, inv, flag.as<int>(), st));
+    int h = 0;
+    MR_CUDA_TRY(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));
+    return h ? MR_ERR_INVALID_PERM : MR_OK;
+}
+
+int mr_csr_validate(const mr_csr_view* A, int* valid, void* stream)
+{
+    if (!valid) return MR_ERR_INVALID_ARG;
+    MR_TRY(check_view(A, false));
+    return validate_csr(*A, valid, as_stream(stream));
+}
+
+int mr_check_perm(const int32_t* perm, int32_t n, int* valid, void* stream)
+{
+    if (!valid || n < 0 || (n > 0 && !perm)) return MR_ERR_INVALID_ARG;
+    return check_perm(perm, n, valid, as_stream(stream));
+}
+
+}  // extern "C"

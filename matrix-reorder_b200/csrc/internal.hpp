@@ -1,0 +1,90 @@
+// Internal declarations shared between the libmr sources.
+#ifndef MR_INTERNAL_HPP
+#define MR_INTERNAL_HPP
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mr.h"
+
+namespace mr {
+
+// MERBIT plan: the reference's descriptor arrays plus the carry scratch.
+struct MerbitPlan {
+    int sigma = 14;
+    int block = 256;
+    int n_rows = 0;
+    int64_t nnz = 0;
+    int lane_num = 0;
+    int tile_num = 0;
+    uint32_t* tile_x = nullptr;   // tile_num + 1
+    uint32_t* tile_y = nullptr;   // tile_num + 1
+    void* lane_desc = nullptr;    // lane_num words (4 or 8 bytes)
+    float* carry = nullptr;       // tile_num carries
+    int device = 0;
+};
+
+int launch_merbit_plan(const int* rowptr, int nrow, int nnz, int sigma, int lane_num, int tile_num, uint32_t* tile_x,
+                       uint32_t* tile_y, void* lane_desc, cudaStream_t st);
+int launch_merbit_spmv(const MerbitPlan& p, const int* colidx, const void* vals, int dtype, const float* x, float* y,
+                       float* carry, cudaStream_t st);
+bool merbit_sigma_supported(int sigma);
+
+int launch_csr_spmv(int n, int64_t nnz, const int* rowptr, const int* colidx, const void* vals, int dtype,
+                    const float* x, float* y, cudaStream_t st);
+
+// permutation
+int permute_csr(const mr_csr_view& A, const int32_t* perm, int32_t* out_rowptr, int32_t* out_colidx, void* out_vals,
+                cudaStream_t st);
+int launch_permute_vector(int n, const int32_t* perm, const float* in, float* out, int inverse, cudaStream_t st);
+int launch_perm_invert(int n, const int32_t* perm, int32_t* inv, int* bad_flag, cudaStream_t st);
+int check_perm(const int32_t* perm, int n, int* valid, cudaStream_t st);
+int validate_csr(const mr_csr_view& A, int* ok, cudaStream_t st);
+
+// device scan: out[i] = sum_{j<i} in[j], out[n] = total (n + 1 outputs)
+int exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t st);
+size_t scan_workspace_bytes(int64_t n);
+int exclusive_scan_i32_ws(const int32_t* in, int32_t* out, int64_t n, void* ws, cudaStream_t st);
+
+// reuse distance
+int rd_hist_exact(const int32_t* stream, int64_t nnz, int32_t ncols, int32_t sector, const int32_t* edges,
+                  int32_t nedges, int64_t* counts, int64_t* valid, cudaStream_t st);
+int rd_hist_sampled(const int32_t* stream, int32_t nnz, int32_t samples, int32_t sector, int32_t rd_cap, int32_t hll_p,
+                    int32_t max_scan, uint32_t seed, const int32_t* edges, int32_t nedges, int64_t* counts,
+                    int64_t* stats, float* est, int32_t* status, int32_t* pos, cudaStream_t st);
+
+// host-side pGOrder
+int pgorder_host(int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_t vsize, int32_t width,
+                 int32_t threads, uint32_t* perm_new2old);
+int32_t pgorder_width(int32_t n, int64_t nnz);
+
+// stream-ordered scratch
+struct DevBuf {
+    void* p = nullptr;
+    cudaStream_t st = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf()
+    {
+        if (p) cudaFreeAsync(p, st);
+    }
+    int alloc(size_t bytes, cudaStream_t s)
+    {
+        st = s;
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMallocAsync(&p, bytes, s);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return MR_ERR_NOMEM;
+        }
+        return MR_OK;
+    }
+    template <typename T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+}  // namespace mr
+
+#endif

@@ -1,0 +1,420 @@
+"""ctypes binding of libmr.so (include/mr.h) and libmr_gen.so.
+
+Python mirror of the library's C-ABI for tests and the benchmark. Device
+buffers are torch CUDA tensors (torch is only the allocator and stream
+provider here); every compute call goes through libmr.so. If the library is
+missing the import of its entry points fails loudly: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBMR_PATH = os.path.join(HERE, "libmr.so")
+LIBGEN_PATH = os.path.join(HERE, "libmr_gen.so")
+
+MR_OK = 0
+MR_ERR_INVALID_ARG = 1
+MR_ERR_CUDA = 2
+MR_ERR_NOMEM = 3
+MR_ERR_INVALID_PERM = 4
+MR_ERR_UNSUPPORTED = 5
+MR_ERR_TIMEOUT = 6
+MR_ERR_BUSY = 7
+MR_ERR_NOT_FOUND = 8
+MR_ERR_INTERNAL = 9
+MR_ERR_PREDICT = 10
+
+MR_F32, MR_F16, MR_BF16 = 0, 1, 2
+MODEL_MERBIT_SAMPLED, MODEL_MERBIT_EXACT, MODEL_CSR_SAMPLED, MODEL_CSR_EXACT = 0, 1, 2, 3
+
+# reference RD bins (src/class.cu:1267)
+REF_EDGES = [1, 112, 512, 18432, 36864, 73728, 147456, 294912, 589824]
+
+
+class MRError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        msg = lib().mr_status_string(code).decode()
+        last = lib().mr_last_error().decode()
+        super().__init__(f"{where}: {msg} ({code})" + (f" [{last}]" if last else ""))
+
+
+class CsrView(C.Structure):
+    _fields_ = [("n_rows", C.c_int32), ("n_cols", C.c_int32), ("nnz", C.c_int64), ("rowptr", C.c_void_p),
+                ("colidx", C.c_void_p), ("vals", C.c_void_p), ("dtype", C.c_int32)]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("sigma", C.c_int32), ("block", C.c_int32), ("n_rows", C.c_int32), ("nnz", C.c_int64),
+                ("lane_num", C.c_int32), ("tile_num", C.c_int32), ("desc_bytes", C.c_int32),
+                ("tile_x_dev", C.c_void_p), ("tile_y_dev", C.c_void_p), ("lane_desc_dev", C.c_void_p)]
+
+
+_lib = None
+_gen = None
+
+
+def _sig(f, res, *args):
+    f.restype = res
+    f.argtypes = list(args)
+
+
+def lib():
+    """Loads libmr.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBMR_PATH):
+        raise RuntimeError(f"{LIBMR_PATH} is missing: run build.py (or __graft_entry__.build())")
+    L = C.CDLL(LIBMR_PATH)
+    vp, i32, i64, u32 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint32
+    P = C.POINTER
+    _sig(L.mr_status_string, C.c_char_p, C.c_int)
+    _sig(L.mr_last_error, C.c_char_p)
+    _sig(L.mr_version, C.c_int)
+    _sig(L.mr_spmv_csr, C.c_int, P(CsrView), vp, vp, vp)
+    _sig(L.mr_merbit_plan_create, C.c_int, P(CsrView), C.c_int, C.c_int, vp, P(vp))
+    _sig(L.mr_merbit_plan_destroy, C.c_int, vp)
+    _sig(L.mr_merbit_plan_get_info, C.c_int, vp, P(PlanInfo))
+    _sig(L.mr_spmv_merbit, C.c_int, vp, P(CsrView), vp, vp, vp)
+    _sig(L.mr_permute_csr, C.c_int, P(CsrView), vp, vp, vp, vp, vp)
+    _sig(L.mr_permute_vector, C.c_int, i32, vp, vp, vp, C.c_int, vp)
+    _sig(L.mr_perm_invert, C.c_int, i32, vp, vp, vp)
+    _sig(L.mr_check_perm, C.c_int, vp, i32, P(C.c_int), vp)
+    _sig(L.mr_predict_speedup, C.c_int, C.c_int, P(C.c_double), P(C.c_double))
+    _sig(L.mr_pgorder_width, i32, i32, i64)
+    _sig(L.mr_pgorder, C.c_int, i32, vp, vp, i32, i32, i32, vp)
+    if hasattr(L, "mr_rd_hist_exact"):
+        _sig(L.mr_rd_hist_exact, C.c_int, vp, i64, i32, i32, vp, i32, vp, vp, vp)
+        _sig(L.mr_rd_hist_sampled, C.c_int, vp, i32, i32, i32, i32, i32, i32, u32, vp, i32, vp, vp, vp, vp, vp, vp)
+        _sig(L.mr_hll_seed, u32, i32, i32)
+        _sig(L.mr_locality_predict, C.c_int, vp, i32, i32, i32, vp, P(C.c_float), vp)
+    if hasattr(L, "mr_graph_create"):
+        _sig(L.mr_graph_create, C.c_int, i32, i64, vp, vp, vp, i32, i32, P(vp))
+        _sig(L.mr_graph_destroy, C.c_int, vp)
+        _sig(L.mr_graph_gorder4, C.c_int, vp, i32, i32, P(C.c_double), P(C.c_double))
+        _sig(L.mr_graph_locality_predict, C.c_int, vp, vp, P(C.c_float))
+        _sig(L.mr_graph_spmv, C.c_int, vp, C.c_char_p, i32, vp, vp, P(C.c_double), P(C.c_double))
+        _sig(L.mr_graph_get_perm, C.c_int, vp, vp)
+        _sig(L.mr_graph_view, C.c_int, vp, P(CsrView))
+    _lib = L
+    return L
+
+
+def check(code: int, where: str) -> None:
+    if code != MR_OK:
+        raise MRError(code, where)
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    return t.data_ptr()
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def torch_dtype_code(t) -> int:
+    import torch
+    return {torch.float32: MR_F32, torch.float16: MR_F16, torch.bfloat16: MR_BF16}[t.dtype]
+
+
+def view(rowptr, colidx, vals, n_cols: Optional[int] = None) -> CsrView:
+    """CsrView over device tensors (int32 rowptr/colidx, f32/f16/bf16 vals)."""
+    n = rowptr.numel() - 1
+    v = CsrView(n, n if n_cols is None else n_cols, colidx.numel(), _ptr(rowptr), _ptr(colidx), _ptr(vals),
+                torch_dtype_code(vals))
+    v._keep = (rowptr, colidx, vals)  # the view owns references to its buffers
+    return v
+
+
+# ---------------------------------------------------------------- SpMV ----
+
+def spmv_csr(A: CsrView, x, y, stream=None) -> None:
+    check(lib().mr_spmv_csr(C.byref(A), _ptr(x), _ptr(y), _stream(stream)), "mr_spmv_csr")
+
+
+class MerbitPlan:
+    """Owner of an mr_merbit_plan (the reference's TILE<BLOCK,SIGMA>)."""
+
+    def __init__(self, A: CsrView, sigma: int = 14, block: int = 256, stream=None):
+        h = C.c_void_p()
+        check(lib().mr_merbit_plan_create(C.byref(A), sigma, block, _stream(stream), C.byref(h)),
+              "mr_merbit_plan_create")
+        self.h = h
+        self.A = A
+
+    def info(self) -> PlanInfo:
+        inf = PlanInfo()
+        check(lib().mr_merbit_plan_get_info(self.h, C.byref(inf)), "mr_merbit_plan_get_info")
+        return inf
+
+    def spmv(self, x, y, A: Optional[CsrView] = None, stream=None) -> None:
+        check(lib().mr_spmv_merbit(self.h, C.byref(A or self.A), _ptr(x), _ptr(y), _stream(stream)),
+              "mr_spmv_merbit")
+
+    def descriptors(self):
+        """Copies (tile_x, tile_y, lane_desc) to host numpy arrays."""
+        import torch
+        inf = self.info()
+        torch.cuda.synchronize()
+        tx = np.empty(inf.tile_num + 1, np.uint32)
+        ty = np.empty(inf.tile_num + 1, np.uint32)
+        dt = np.uint32 if inf.desc_bytes == 4 else np.uint64
+        ld = np.empty(inf.lane_num, dt)
+        for arr, p in ((tx, inf.tile_x_dev), (ty, inf.tile_y_dev), (ld, inf.lane_desc_dev)):
+            _d2h(arr, p)
+        return tx, ty, ld
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().mr_merbit_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _DevArray:
+    """Minimal __cuda_array_interface__ holder so torch can view a raw device pointer."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 2, "strides": None}
+
+
+def dev_view(ptr: int, nbytes: int):
+    """uint8 torch tensor aliasing nbytes of device memory at ptr (no copy)."""
+    import torch
+    return torch.as_tensor(_DevArray(ptr, nbytes), device="cuda")
+
+
+def _d2h(arr: np.ndarray, dev_ptr: int) -> None:
+    """Copies arr.nbytes from a raw device pointer into arr."""
+    if arr.nbytes == 0:
+        return
+    arr.view(np.uint8)[:] = dev_view(dev_ptr, arr.nbytes).cpu().numpy()
+
+
+# ---------------------------------------------------------- permutation ----
+
+def permute_csr(A: CsrView, perm, out_rowptr, out_colidx, out_vals, stream=None) -> None:
+    check(lib().mr_permute_csr(C.byref(A), _ptr(perm), _ptr(out_rowptr), _ptr(out_colidx), _ptr(out_vals),
+                               _stream(stream)), "mr_permute_csr")
+
+
+def permute_vector(perm, inp, out, inverse: bool, stream=None) -> None:
+    check(lib().mr_permute_vector(perm.numel(), _ptr(perm), _ptr(inp), _ptr(out), int(inverse), _stream(stream)),
+          "mr_permute_vector")
+
+
+def perm_invert(perm, inv, stream=None) -> None:
+    check(lib().mr_perm_invert(perm.numel(), _ptr(perm), _ptr(inv), _stream(stream)), "mr_perm_invert")
+
+
+def check_perm(perm, stream=None) -> bool:
+    v = C.c_int(0)
+    check(lib().mr_check_perm(_ptr(perm), perm.numel(), C.byref(v), _stream(stream)), "mr_check_perm")
+    return bool(v.value)
+
+
+# -------------------------------------------------------- RD / predictor ----
+
+def rd_hist_exact(stream_dev, ncols: int, sector: int = 32, edges=REF_EDGES, stream=None):
+    e = np.asarray(edges, np.int32)
+    counts = np.zeros(len(e) + 1, np.int64)
+    valid = np.zeros(1, np.int64)
+    check(lib().mr_rd_hist_exact(_ptr(stream_dev), stream_dev.numel(), ncols, sector, e.ctypes.data, len(e),
+                                 counts.ctypes.data, valid.ctypes.data, _stream(stream)), "mr_rd_hist_exact")
+    return counts, int(valid[0])
+
+
+def rd_hist_sampled(stream_dev, samples: int = 30960, sector: int = 32, rd_cap: int = 589824, hll_p: int = 12,
+                    max_scan: int = 0, seed: int = 246813579, edges=REF_EDGES, est=None, status=None, pos=None,
+                    stream=None):
+    e = np.asarray(edges, np.int32)
+    counts = np.zeros(len(e) + 1, np.int64)
+    stats = np.zeros(4, np.int64)
+    check(lib().mr_rd_hist_sampled(_ptr(stream_dev), stream_dev.numel(), samples, sector, rd_cap, hll_p, max_scan,
+                                   seed, e.ctypes.data, len(e), counts.ctypes.data, stats.ctypes.data, _ptr(est),
+                                   _ptr(status), _ptr(pos), _stream(stream)), "mr_rd_hist_sampled")
+    return counts, stats
+
+
+def hll_seed(graph_id: int, stream_type: int = 0) -> int:
+    return int(lib().mr_hll_seed(graph_id, stream_type))
+
+
+def predict_speedup(features, model: int = MODEL_MERBIT_SAMPLED) -> float:
+    r = (C.c_double * 10)(*[float(v) for v in features])
+    out = C.c_double(0)
+    check(lib().mr_predict_speedup(model, r, C.byref(out)), "mr_predict_speedup")
+    return out.value
+
+
+def locality_predict(stream_dev, ncols: int, graph_id: int = 0, stream=None):
+    f = np.zeros(10, np.float64)
+    s = C.c_float(0)
+    check(lib().mr_locality_predict(_ptr(stream_dev), stream_dev.numel(), ncols, graph_id, f.ctypes.data,
+                                    C.byref(s), _stream(stream)), "mr_locality_predict")
+    return s.value, f
+
+
+# -------------------------------------------------------------- pGOrder ----
+
+def pgorder_width(n: int, nnz: int) -> int:
+    return int(lib().mr_pgorder_width(n, nnz))
+
+
+def pgorder(rowptr: np.ndarray, colidx: np.ndarray, vsize: int = 0, width: int = 5, threads: int = 0) -> np.ndarray:
+    """Host pGOrder: returns perm_new2old (uint32)."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    colidx = np.ascontiguousarray(colidx, np.int32)
+    n = rowptr.size - 1
+    out = np.empty(n, np.uint32)
+    check(lib().mr_pgorder(n, rowptr.ctypes.data, colidx.ctypes.data, vsize, width, threads, out.ctypes.data),
+          "mr_pgorder")
+    return out
+
+
+# ------------------------------------------------------------ GRAPH object ----
+
+class Graph:
+    """Mirror of the reference's GRAPH<float> operator API over mr_graph."""
+
+    def __init__(self, rowptr: np.ndarray, colidx: np.ndarray, vals: np.ndarray, graph_id: int = 0):
+        rowptr = np.ascontiguousarray(rowptr, np.int32)
+        colidx = np.ascontiguousarray(colidx, np.int32)
+        if vals.dtype == np.float32:
+            dt = MR_F32
+        elif vals.dtype == np.float16:
+            dt = MR_F16
+        else:
+            raise ValueError("vals must be float32 or float16 (bf16 via the C-ABI directly)")
+        vals = np.ascontiguousarray(vals)
+        h = C.c_void_p()
+        check(lib().mr_graph_create(rowptr.size - 1, colidx.size, rowptr.ctypes.data, colidx.ctypes.data,
+                                    vals.ctypes.data, dt, graph_id, C.byref(h)), "mr_graph_create")
+        self.h = h
+        self.n = rowptr.size - 1
+
+    def gorder4(self, vsize: int = 0, width: int = 5):
+        a, b = C.c_double(0), C.c_double(0)
+        check(lib().mr_graph_gorder4(self.h, vsize, width, C.byref(a), C.byref(b)), "mr_graph_gorder4")
+        return a.value, b.value
+
+    def locality_predict(self):
+        f = np.zeros(10, np.float64)
+        s = C.c_float(0)
+        check(lib().mr_graph_locality_predict(self.h, f.ctypes.data, C.byref(s)), "mr_graph_locality_predict")
+        return s.value, f
+
+    def spmv(self, method: str = "merbit", iters: int = 1, x: Optional[np.ndarray] = None):
+        y = np.empty(self.n, np.float32)
+        xp = None if x is None else np.ascontiguousarray(x, np.float32)
+        a, b = C.c_double(0), C.c_double(0)
+        check(lib().mr_graph_spmv(self.h, method.encode(), iters, None if xp is None else xp.ctypes.data,
+                                  y.ctypes.data, C.byref(a), C.byref(b)), "mr_graph_spmv")
+        return y, a.value, b.value
+
+    def perm(self) -> np.ndarray:
+        p = np.empty(self.n, np.int32)
+        check(lib().mr_graph_get_perm(self.h, p.ctypes.data), "mr_graph_get_perm")
+        return p
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mr_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ----------------------------------------------------------- generators ----
+
+def gen():
+    global _gen
+    if _gen is not None:
+        return _gen
+    if not os.path.exists(LIBGEN_PATH):
+        raise RuntimeError(f"{LIBGEN_PATH} is missing: run build.py")
+    G = C.CDLL(LIBGEN_PATH)
+    vp = C.c_void_p
+    _sig(G.mrg_rmat, vp, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int)
+    _sig(G.mrg_laplace2d, vp, C.c_int32, C.c_int, C.c_uint64)
+    _sig(G.mrg_chung_lu, vp, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_uint64)
+    _sig(G.mrg_banded, vp, C.c_int32, C.c_int32, C.c_uint64)
+    _sig(G.mrg_n, C.c_int32, vp)
+    _sig(G.mrg_nnz, C.c_int64, vp)
+    _sig(G.mrg_copy, None, vp, vp, vp, vp)
+    _sig(G.mrg_free, None, vp)
+    _sig(G.mrg_uniform, None, C.c_uint64, C.c_int64, vp)
+    _sig(G.mrg_random_perm, None, C.c_int32, C.c_uint64, vp)
+    _sig(G.mrg_threads, C.c_int)
+    _gen = G
+    return G
+
+
+def _take(h):
+    G = gen()
+    if not h:
+        raise ValueError("generator rejected its arguments")
+    n, nnz = G.mrg_n(h), G.mrg_nnz(h)
+    rp = np.empty(n + 1, np.int32)
+    ci = np.empty(nnz, np.int32)
+    v = np.empty(nnz, np.float32)
+    G.mrg_copy(h, rp.ctypes.data, ci.ctypes.data, v.ctypes.data)
+    G.mrg_free(h)
+    return rp, ci, v
+
+
+def gen_rmat(scale: int = 16, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 1, permute_ids=True,
+             n: Optional[int] = None):
+    """Graph500 R-MAT CSR (duplicates merged, self loops kept), values U[-1,1]."""
+    n = (1 << scale) if n is None else n
+    return _take(gen().mrg_rmat(n, edge_factor, a, b, c, seed, int(permute_ids)))
+
+
+def gen_laplace2d(g: int = 2048, shuffle: bool = True, seed: int = 1):
+    return _take(gen().mrg_laplace2d(g, int(shuffle), seed))
+
+
+def gen_chung_lu(n: int, gamma=2.1, mean_deg=20.0, dmin=1, dmax=200000, seed: int = 1):
+    return _take(gen().mrg_chung_lu(n, gamma, mean_deg, dmin, dmax, seed))
+
+
+def gen_banded(n: int, bandwidth: int, seed: int = 1):
+    return _take(gen().mrg_banded(n, bandwidth, seed))
+
+
+def uniform(count: int, seed: int) -> np.ndarray:
+    out = np.empty(count, np.float32)
+    gen().mrg_uniform(seed, count, out.ctypes.data)
+    return out
+
+
+def random_perm(n: int, seed: int) -> np.ndarray:
+    out = np.empty(n, np.int32)
+    gen().mrg_random_perm(n, seed, out.ctypes.data)
+    return out

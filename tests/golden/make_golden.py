@@ -1,0 +1,68 @@
+"""Generates the host-side golden fixtures from the reference's own code.
+
+Runs the reference functions compiled from its sources (oracle/_ref, built by
+oracle/build_ref.sh from the reference checkout) on small seeded inputs and
+stores inputs and outputs in tests/golden/golden_host.npz:
+
+  * pGOrder permutations (order_on_cpu driven as GRAPH::gorder4 does,
+    src/class.cu:2647-2683),
+  * exact RD bin probabilities (compute_sector_rd_histogram,
+    src/class.cu:892-936) for the reference bins and log2 bins,
+  * GRAPH::get_width over a grid of sizes (src/class.cu:733-750),
+  * rd_merbit_model::PredictSpeedup on feature vectors (include/model.cuh).
+
+Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+sys.path.insert(0, os.path.join(REPO, "matrix-reorder_b200"))
+
+import mrb200 as M  # noqa: E402  (generators only)
+import pyoracle as O  # noqa: E402
+
+LOG2_EDGES = [1 << k for k in range(0, 13)]
+
+
+def main() -> None:
+    assert O.ref_available(), "build oracle/_ref first (oracle/build_ref.sh)"
+    out = {}
+    cases = {
+        "rmat12": M.gen_rmat(scale=12, edge_factor=8, seed=3)[:2],
+        "lap24": M.gen_laplace2d(24, shuffle=True, seed=5)[:2],
+        "band": M.gen_banded(3000, 9, seed=2)[:2],
+    }
+    for name, (rp, ci) in cases.items():
+        n = rp.size - 1
+        out[f"{name}_rowptr"] = rp
+        out[f"{name}_colidx"] = ci
+        for vs in (1024, 256, 64):
+            out[f"{name}_perm_v{vs}_w5"] = O.ref_pgorder(rp, ci, vs, 5)
+        out[f"{name}_perm_v256_w1"] = O.ref_pgorder(rp, ci, 256, 1)
+        out[f"{name}_rd_ref"] = O.ref_rd_probs(ci, n, 32)
+        out[f"{name}_rd_log2"] = O.ref_rd_probs(ci, n, 32, LOG2_EDGES)
+        out[f"{name}_rd_s8"] = O.ref_rd_probs(ci, n, 8)
+    sizes = []
+    for n in (1000, 4096, 65536, 1 << 20, 4194304, 8388608, 16777216):
+        for deg in (1, 2, 3, 4, 5, 8, 16, 20, 64, 200):
+            if n * deg < 2**31:  # the reference takes int sizes
+                sizes.append((n, n * deg))
+    sizes.append((100, 50))  # nnz / n == 0
+    sizes = np.array(sizes, np.int64)
+    out["width_sizes"] = sizes
+    out["width_ref"] = np.array([O.ref_get_width(int(a), int(b)) for a, b in sizes], np.int32)
+    rng = np.random.default_rng(11)
+    feats = rng.dirichlet(np.ones(10), size=16)
+    out["predict_features"] = feats
+    out["predict_ref"] = np.array([O.ref_predict(f) for f in feats])
+    np.savez_compressed(os.path.join(HERE, "golden_host.npz"), **out)
+    print("wrote", os.path.join(HERE, "golden_host.npz"))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,209 @@
+"""GPU parity of the SpMV path: MERBIT plan descriptors (bit-exact against the
+oracle's restatement of Tile_Kernel and, when built, the reference kernel
+itself), MERBIT and plain CSR SpMV against the FP64 oracle (relative L2
+<= 1e-5 for FP32 values), determinism, dtypes and edge cases."""
+import numpy as np
+import pytest
+
+from conftest import csr_from_dense_pattern, csr_random
+
+pytestmark = pytest.mark.gpu
+
+REL_L2_F32 = 1e-5
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _rel_l2(got, ref):
+    ref = np.asarray(ref, np.float64)
+    d = np.linalg.norm(np.asarray(got, np.float64) - ref)
+    nr = np.linalg.norm(ref)
+    return d / nr if nr > 0 else d
+
+
+def _plan_and_spmv(M, rp, ci, v, x, sigma=14, block=256, dtype=None):
+    import torch
+    vals = _dev(v)
+    if dtype is not None:
+        vals = vals.to(dtype)
+    ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+    A = M.view(_dev(rp), _dev(ci), vals, n_cols=ncols)
+    keep = (A, vals)
+    plan = M.MerbitPlan(A, sigma=sigma, block=block)
+    xd = _dev(x)
+    y = torch.full((rp.size - 1,), float("nan"), device="cuda")
+    plan.spmv(xd, y)
+    torch.cuda.synchronize()
+    return plan, y.cpu().numpy(), keep
+
+
+def _edge_cases():
+    rng = np.random.default_rng(0)
+    cases = {
+        "one_row": csr_from_dense_pattern([[0]]),
+        "one_row_empty": csr_from_dense_pattern([[]]),
+        "all_empty": csr_from_dense_pattern([[] for _ in range(1000)]),
+        "single_nnz": csr_from_dense_pattern([[] for _ in range(500)] + [[7]] + [[] for _ in range(499)]),
+        "huge_row": csr_from_dense_pattern([sorted(rng.choice(60000, 50000, replace=False).tolist())] +
+                                           [[i] for i in range(1, 300)]),
+        "rows_fill_lane": csr_from_dense_pattern([[j for j in range(13)] for _ in range(700)]),
+        "rows_fill_tile": csr_from_dense_pattern([[j for j in range(447)] for _ in range(40)]),
+        "rows_fill_block": csr_from_dense_pattern([[j for j in range(3583)] for _ in range(6)]),
+        "random_small": csr_random(3000, 40, seed=1, empty_frac=0.2),
+        "random_wide": csr_random(2000, 300, seed=2, ncols=5000, empty_frac=0.5),
+    }
+    return cases
+
+
+@pytest.fixture(scope="module")
+def cases(M):
+    c = _edge_cases()
+    rp, ci, v = M.gen_rmat(scale=13, edge_factor=16, seed=4)
+    c["rmat13"] = (rp, ci, v)
+    rp, ci, v = M.gen_laplace2d(64, shuffle=True, seed=3)
+    c["lap64"] = (rp, ci, v)
+    return c
+
+
+@pytest.mark.parametrize("sigma", [7, 14, 16, 32])
+def test_plan_descriptors_match_oracle(M, O, cases, sigma):
+    for name, (rp, ci, v) in cases.items():
+        plan, _, _ = _plan_and_spmv(M, rp, ci, v, np.ones(max(rp.size - 1, int(ci.max(initial=0)) + 1), np.float32),
+                                    sigma=sigma)
+        tx, ty, ld = plan.descriptors()
+        otx, oty, old = O.merbit_plan(rp, ci.size, sigma)
+        assert np.array_equal(tx, otx), (name, sigma, "tile_x")
+        assert np.array_equal(ty, oty), (name, sigma, "tile_y")
+        assert np.array_equal(ld, old), (name, sigma, "lane_desc")
+        plan.close()
+
+
+def test_plan_descriptors_match_reference_kernel(M, O, cases):
+    R = O.ref()
+    if R is None:
+        pytest.skip("reference build (oracle/_ref) not present")
+    import torch
+    for name, (rp, ci, v) in cases.items():
+        n = rp.size - 1
+        plan, _, _ = _plan_and_spmv(M, rp, ci, v, np.ones(max(n, int(ci.max(initial=0)) + 1), np.float32))
+        tx, ty, ld = plan.descriptors()
+        rtx = torch.zeros(tx.size, dtype=torch.int32, device="cuda")
+        rty = torch.zeros(ty.size, dtype=torch.int32, device="cuda")
+        rld = torch.zeros(max(ld.size, 1), dtype=torch.int32, device="cuda")
+        rpd = _dev(rp)
+        assert R.ref_tile_build(rpd.data_ptr(), n, int(ci.size), rtx.data_ptr(), rty.data_ptr(), rld.data_ptr()) == 0
+        assert np.array_equal(tx, rtx.cpu().numpy().view(np.uint32)), name
+        assert np.array_equal(ty, rty.cpu().numpy().view(np.uint32)), name
+        assert np.array_equal(ld, rld.cpu().numpy().view(np.uint32)[:ld.size]), name
+        plan.close()
+
+
+@pytest.mark.parametrize("sigma", [7, 10, 14, 16, 20, 24, 28, 32])
+def test_merbit_spmv_matches_fp64(M, O, cases, sigma):
+    for name, (rp, ci, v) in cases.items():
+        ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+        x = M.uniform(ncols, seed=11)
+        plan, y, _ = _plan_and_spmv(M, rp, ci, v, x, sigma=sigma)
+        ref = O.spmv_f64(rp, ci, v, x)
+        assert not np.isnan(y).any(), (name, sigma)
+        assert _rel_l2(y, ref) <= REL_L2_F32, (name, sigma, _rel_l2(y, ref))
+        plan.close()
+
+
+@pytest.mark.parametrize("block", [128, 256, 512])
+def test_merbit_block_sizes(M, O, cases, block):
+    rp, ci, v = cases["rmat13"]
+    x = M.uniform(rp.size - 1, seed=5)
+    plan, y, _ = _plan_and_spmv(M, rp, ci, v, x, block=block)
+    assert _rel_l2(y, O.spmv_f64(rp, ci, v, x)) <= REL_L2_F32
+    plan.close()
+
+
+def test_merbit_is_deterministic(M, cases):
+    import torch
+    rp, ci, v = cases["huge_row"]
+    ncols = int(ci.max()) + 1
+    x = M.uniform(ncols, seed=3)
+    vals = _dev(v)
+    A = M.view(_dev(rp), _dev(ci), vals, n_cols=ncols)
+    plan = M.MerbitPlan(A)
+    xd = _dev(x)
+    y1 = torch.empty(rp.size - 1, device="cuda")
+    y2 = torch.empty(rp.size - 1, device="cuda")
+    plan.spmv(xd, y1)
+    for _ in range(3):
+        plan.spmv(xd, y2)
+    torch.cuda.synchronize()
+    assert torch.equal(y1.view(torch.int32), y2.view(torch.int32))
+    plan.close()
+
+
+@pytest.mark.parametrize("tdt", ["float16", "bfloat16"])
+def test_merbit_half_values(M, O, cases, tdt):
+    import torch
+    dt = getattr(torch, tdt)
+    for name in ("rmat13", "huge_row", "random_small"):
+        rp, ci, v = cases[name]
+        ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+        x = M.uniform(ncols, seed=13)
+        plan, y, _ = _plan_and_spmv(M, rp, ci, v, x, dtype=dt)
+        v_rounded = torch.from_numpy(v).to(dt).float().numpy()
+        assert _rel_l2(y, O.spmv_f64(rp, ci, v_rounded, x)) <= REL_L2_F32, (name, tdt)
+        plan.close()
+
+
+def test_merbit_vs_reference_kernel(M, O, cases):
+    R = O.ref()
+    if R is None:
+        pytest.skip("reference build (oracle/_ref) not present")
+    import ctypes
+    import torch
+    for name in ("rmat13", "lap64", "random_small", "rows_fill_tile"):
+        rp, ci, v = cases[name]
+        n = rp.size - 1
+        x = M.uniform(max(n, int(ci.max(initial=0)) + 1), seed=21)
+        plan, y, _ = _plan_and_spmv(M, rp, ci, v, x)
+        inf = plan.info()
+        yr = torch.zeros(n, device="cuda")
+        zr = torch.zeros(n, device="cuda")
+        rpd, cid, vd, xd = _dev(rp), _dev(ci), _dev(v), _dev(x)
+        ms = ctypes.c_float(0)
+        assert R.ref_merbit_spmv(rpd.data_ptr(), cid.data_ptr(), vd.data_ptr(), n, int(ci.size), inf.tile_x_dev,
+                                 inf.tile_y_dev, inf.lane_desc_dev, xd.data_ptr(), yr.data_ptr(), zr.data_ptr(), 3,
+                                 ctypes.byref(ms)) == 0
+        ref64 = O.spmv_f64(rp, ci, v, x)
+        assert _rel_l2(yr.cpu().numpy(), ref64) <= REL_L2_F32, name
+        assert _rel_l2(y, yr.cpu().numpy()) <= 2 * REL_L2_F32, name
+        plan.close()
+
+
+@pytest.mark.parametrize("tdt", ["float32", "float16", "bfloat16"])
+def test_csr_spmv_matches_fp64(M, O, cases, tdt):
+    import torch
+    dt = getattr(torch, tdt)
+    for name, (rp, ci, v) in cases.items():
+        ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+        x = M.uniform(ncols, seed=17)
+        vals = _dev(v).to(dt)
+        A = M.view(_dev(rp), _dev(ci), vals, n_cols=ncols)
+        y = torch.full((rp.size - 1,), float("nan"), device="cuda")
+        M.spmv_csr(A, _dev(x), y)
+        torch.cuda.synchronize()
+        vr = vals.float().cpu().numpy()
+        assert _rel_l2(y.cpu().numpy(), O.spmv_f64(rp, ci, vr, x)) <= REL_L2_F32, (name, tdt)
+
+
+def test_plan_rejects_mismatched_matrix(M, cases):
+    rp, ci, v = cases["rmat13"]
+    A = M.view(_dev(rp), _dev(ci), _dev(v))
+    plan = M.MerbitPlan(A)
+    rp2, ci2, v2 = cases["lap64"]
+    B = M.view(_dev(rp2), _dev(ci2), _dev(v2))
+    import torch
+    with pytest.raises(M.MRError) as e:
+        plan.spmv(_dev(np.ones(rp2.size - 1, np.float32)), torch.empty(rp2.size - 1, device="cuda"), A=B)
+    assert e.value.code == M.MR_ERR_INVALID_ARG
+    plan.close()
