@@ -208,4 +208,54 @@ int mr_check_perm(const int32_t* perm, int32_t n, int* valid, void* stream)
     return check_perm(perm, n, valid, as_stream(stream));
 }
 
+static int check_edges(const int32_t* edges, int32_t nedges)
+{
+    if (!edges || nedges < 1 || nedges > 63) return MR_ERR_INVALID_ARG;
+    for (int i = 1; i < nedges; ++i)
+        if (edges[i] < edges[i - 1]) return MR_ERR_INVALID_ARG;
+    return MR_OK;
+}
+
+int mr_rd_hist_exact(const int32_t* s, int64_t nnz, int32_t ncols, int32_t sector, const int32_t* edges,
+                     int32_t nedges, int64_t* counts, int64_t* valid, void* stream)
+{
+    if (nnz < 0 || nnz > INT32_MAX || ncols < 0 || sector <= 0 || !counts || !valid || (nnz > 0 && !s))
+        return MR_ERR_INVALID_ARG;
+    MR_TRY(check_edges(edges, nedges));
+    return rd_hist_exact(s, nnz, ncols, sector, edges, nedges, counts, valid, as_stream(stream));
+}
+
+int mr_rd_hist_sampled(const int32_t* s, int32_t nnz, int32_t samples, int32_t sector, int32_t rd_cap, int32_t hll_p,
+                       int32_t max_scan, uint32_t seed, const int32_t* edges, int32_t nedges, int64_t* counts,
+                       int64_t* stats, float* est, int32_t* status, int32_t* pos, void* stream)
+{
+    // argument rules of sampled_hll_rd_block_gpu (src/class.cu:1149-1167)
+    if (!counts || !stats || nnz < 0 || (nnz > 1 && !s)) return MR_ERR_INVALID_ARG;
+    if (sector <= 0) return MR_ERR_INVALID_ARG;
+    MR_TRY(check_edges(edges, nedges));
+    if (rd_cap > 0 && rd_cap < edges[nedges - 1]) return MR_ERR_INVALID_ARG;
+    return rd_hist_sampled(s, nnz, samples, sector, rd_cap, hll_p, max_scan, seed, edges, nedges, counts, stats, est,
+                           status, pos, as_stream(stream));
+}
+
+int mr_locality_predict(const int32_t* s, int32_t nnz, int32_t ncols, int32_t graph_id, double* features10,
+                        float* speedup, void* stream)
+{
+    // settings of GRAPH::locality_predict (src/class.cu:1265-1277)
+    static const int32_t kEdges[9] = {1, 112, 512, 18432, 36864, 73728, 147456, 294912, 589824};
+    if (!speedup || ncols < 0) return MR_ERR_INVALID_ARG;
+    int64_t counts[10], stats[4];
+    MR_TRY(mr_rd_hist_sampled(s, nnz, 30960, 32, kEdges[8], 12, 0, mr_hll_seed(graph_id, 0), kEdges, 9, counts, stats,
+                              nullptr, nullptr, nullptr, stream));
+    double f[10];
+    const int64_t valid = stats[0] + stats[2];  // found + large
+    for (int i = 0; i < 10; ++i) f[i] = valid > 0 ? (double)counts[i] / (double)valid : 0.0;
+    if (features10)
+        for (int i = 0; i < 10; ++i) features10[i] = f[i];
+    double sp = 0.0;
+    const int rc = mr_predict_speedup(MR_MODEL_MERBIT_SAMPLED, f, &sp);
+    *speedup = (float)sp;
+    return rc;
+}
+
 }  // extern "C"

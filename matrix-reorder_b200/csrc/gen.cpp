@@ -17,6 +17,8 @@
 #include <cstring>
 #include <numeric>
 #include <random>
+#include <cstdio>
+#include <string>
 #include <vector>
 #include <omp.h>
 
@@ -339,6 +341,128 @@ int mrg_relabel(mrg_csr* m, const int32_t* perm_old2new)
     if (!m) return 1;
     relabel(m, std::vector<int32_t>(perm_old2new, perm_old2new + m->n));
     return 0;
+}
+
+// Matrix Market reader with the reference's semantics (BASEGRAPH ctor,
+// src/class.cu:5-73): "symmetric" in the banner line doubles every entry
+// (the mirrored copies are appended after the Nnz listed ones, diagonal
+// entries included); "basezero" in the banner means 0-based indices; values
+// are forced to 1.0 unless keep_values. The reference multiplies the
+// transpose of the file's matrix (its col_ind is the SpMV row, :1342), so the
+// CSR returned here has row = file column and column = file row, sorted by
+// (row, column) with duplicates kept in file order. Blank lines are skipped.
+// *err: 0 ok, 1 cannot open, 2 bad header, 3 bad entry / index out of range.
+mrg_csr* mrg_read_mtx(const char* path, int keep_values, int* err)
+{
+    auto fail = [&](int e) -> mrg_csr* { if (err) *err = e; return nullptr; };
+    FILE* f = std::fopen(path, "r");
+    if (!f) return fail(1);
+    std::vector<char> line(1 << 16);
+    bool first = true, symmetric = false, zero_base = false;
+    long long R = -1, Cc = -1, N = -1;
+    while (std::fgets(line.data(), (int)line.size(), f)) {
+        std::string l(line.data());
+        if (first) {
+            symmetric = l.find("symmetric") != std::string::npos;
+            zero_base = l.find("basezero") != std::string::npos;
+            first = false;
+        }
+        if (!l.empty() && l[0] == '%') continue;
+        if (std::sscanf(l.c_str(), "%lld %lld %lld", &R, &Cc, &N) == 3) break;
+        if (l.find_first_not_of(" \t\r\n") == std::string::npos) continue;
+        std::fclose(f);
+        return fail(2);
+    }
+    if (R < 0 || Cc < 0 || N < 0 || R > INT32_MAX || Cc > INT32_MAX || (symmetric ? 2 * N : N) > INT32_MAX) {
+        std::fclose(f);
+        return fail(2);
+    }
+    const int64_t total = symmetric ? 2 * N : N;
+    std::vector<int32_t> rows((size_t)total), cols((size_t)total);
+    std::vector<float> vals(keep_values ? (size_t)total : 0);
+    int64_t i = 0;
+    const int32_t n = (int32_t)std::max(R, Cc);
+    while (i < N && std::fgets(line.data(), (int)line.size(), f)) {
+        long long r, c;
+        double v = 1.0;
+        const int k = std::sscanf(line.data(), "%lld %lld %lf", &r, &c, &v);
+        if (k < 2) continue;  // blank or comment line
+        if (!zero_base) { --r; --c; }
+        if (r < 0 || c < 0 || r >= n || c >= n) { std::fclose(f); return fail(3); }
+        // SpMV row = file column, SpMV column = file row
+        rows[(size_t)i] = (int32_t)c;
+        cols[(size_t)i] = (int32_t)r;
+        if (keep_values) vals[(size_t)i] = (float)v;
+        if (symmetric) {
+            rows[(size_t)(N + i)] = (int32_t)r;
+            cols[(size_t)(N + i)] = (int32_t)c;
+            if (keep_values) vals[(size_t)(N + i)] = (float)v;
+        }
+        ++i;
+    }
+    std::fclose(f);
+    if (i != N) return fail(3);
+    // counting sort by row (stable in file order), then stable sort by column
+    auto* m = new mrg_csr;
+    m->n = n;
+    m->rowptr.assign((size_t)n + 1, 0);
+    for (int64_t e = 0; e < total; ++e) ++m->rowptr[(size_t)rows[(size_t)e] + 1];
+    for (int32_t r = 0; r < n; ++r) m->rowptr[(size_t)r + 1] += m->rowptr[(size_t)r];
+    std::vector<int32_t> fill(m->rowptr.begin(), m->rowptr.end() - 1);
+    std::vector<int64_t> src((size_t)total);
+    for (int64_t e = 0; e < total; ++e) src[(size_t)fill[(size_t)rows[(size_t)e]]++] = e;
+    m->colidx.resize((size_t)total);
+    m->vals.resize((size_t)total);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int32_t r = 0; r < n; ++r) {
+        auto b = src.begin() + m->rowptr[(size_t)r], e = src.begin() + m->rowptr[(size_t)r + 1];
+        std::stable_sort(b, e, [&](int64_t a, int64_t q) { return cols[(size_t)a] < cols[(size_t)q]; });
+        for (auto it = b; it != e; ++it) {
+            const size_t k = (size_t)(it - src.begin());
+            m->colidx[k] = cols[(size_t)*it];
+            m->vals[k] = keep_values ? vals[(size_t)*it] : 1.0f;
+        }
+    }
+    if (err) *err = 0;
+    return m;
+}
+
+// The reference's controlled perturbation local_swap (src/class.cu:236-301):
+// rho*n seeded swaps of i with a j drawn from [i-window, i-near] or
+// [i+near, i+window] (side chosen in proportion to the lengths). Uses the
+// same standard-library engine and distributions, so a given seed gives the
+// reference's permutation on the same C++ standard library.
+void mrg_local_swap(int32_t n, float rho, int32_t near_, int32_t window, uint64_t seed, int32_t* permutation)
+{
+    std::mt19937_64 rng(seed);
+    const int n_swaps = (int)std::llround(rho * (double)n);
+    std::vector<int> list((size_t)n);
+    std::iota(list.begin(), list.end(), 0);
+    std::shuffle(list.begin(), list.end(), rng);
+    list.resize((size_t)n_swaps);
+    for (int i : list) {
+        const int l1 = std::max(0, i - window), r1 = std::min(n - 1, i - near_);
+        const int l2 = std::max(0, i + near_), r2 = std::min(n - 1, i + window);
+        const int len1 = (l1 <= r1) ? (r1 - l1 + 1) : 0;
+        const int len2 = (l2 <= r2) ? (r2 - l2 + 1) : 0;
+        if (len1 + len2 == 0) continue;
+        bool left;
+        if (len1 > 0 && len2 > 0) {
+            std::bernoulli_distribution pick(double(len1) / double(len1 + len2));
+            left = pick(rng);
+        } else {
+            left = len1 > 0;
+        }
+        int j;
+        if (left) {
+            std::uniform_int_distribution<int> u(l1, r1);
+            j = u(rng);
+        } else {
+            std::uniform_int_distribution<int> u(l2, r2);
+            j = u(rng);
+        }
+        if (j != i) std::swap(permutation[i], permutation[j]);
+    }
 }
 
 int32_t mrg_n(const mrg_csr* m) { return m ? m->n : 0; }

@@ -21,6 +21,12 @@ mrg_csr* mrg_banded(int32_t n, int32_t bandwidth, uint64_t seed);
 mrg_csr* mrg_from_csr(int32_t n, const int32_t* rowptr, const int32_t* colidx, const float* vals);
 int mrg_relabel(mrg_csr* m, const int32_t* perm_old2new);
 
+/* Matrix Market file with the reference's reader semantics (see gen.cpp);
+ * returns the CSR the reference multiplies. *err: 0 ok, 1 open, 2 header,
+ * 3 entries. */
+mrg_csr* mrg_read_mtx(const char* path, int keep_values, int* err);
+/* The reference's local_swap perturbation of `permutation` (in place). */
+void mrg_local_swap(int32_t n, float rho, int32_t near_, int32_t window, uint64_t seed, int32_t* permutation);
 int32_t mrg_n(const mrg_csr* m);
 int64_t mrg_nnz(const mrg_csr* m);
 const int32_t* mrg_rowptr(const mrg_csr* m);

@@ -372,6 +372,8 @@ def gen():
     _sig(G.mrg_uniform, None, C.c_uint64, C.c_int64, vp)
     _sig(G.mrg_random_perm, None, C.c_int32, C.c_uint64, vp)
     _sig(G.mrg_threads, C.c_int)
+    _sig(G.mrg_read_mtx, vp, C.c_char_p, C.c_int, C.POINTER(C.c_int))
+    _sig(G.mrg_local_swap, None, C.c_int32, C.c_float, C.c_int32, C.c_int32, C.c_uint64, vp)
     _gen = G
     return G
 
@@ -406,6 +408,22 @@ def gen_chung_lu(n: int, gamma=2.1, mean_deg=20.0, dmin=1, dmax=200000, seed: in
 
 def gen_banded(n: int, bandwidth: int, seed: int = 1):
     return _take(gen().mrg_banded(n, bandwidth, seed))
+
+
+def read_mtx(path: str, keep_values: bool = False):
+    """Matrix Market file as the CSR the reference multiplies (see gen.cpp)."""
+    err = C.c_int(0)
+    h = gen().mrg_read_mtx(path.encode(), int(keep_values), C.byref(err))
+    if not h:
+        raise ValueError(f"cannot read {path}: error {err.value}")
+    return _take(h)
+
+
+def local_swap(n: int, rho: float, near: int, window: int, seed: int) -> np.ndarray:
+    """The reference's local_swap perturbation of the identity permutation."""
+    p = np.arange(n, dtype=np.int32)
+    gen().mrg_local_swap(n, rho, near, window, seed, p.ctypes.data)
+    return p
 
 
 def uniform(count: int, seed: int) -> np.ndarray:

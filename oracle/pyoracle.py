@@ -68,6 +68,7 @@ def ref():
         _sig(L.ref_rd_hist_exact, None, vp, i32, i32, i32, vp, i32, vp)
         _sig(L.ref_pgorder_host, None, i32, vp, vp, vp, vp, i32, i32, vp)
         _sig(L.ref_predict, C.c_double, vp)
+        _sig(L.ref_local_swap, None, i32, C.c_float, i32, i32, C.c_ulonglong, vp)
         _sig(L.ref_tile_build, C.c_int, vp, i32, i32, vp, vp, vp)
         _sig(L.ref_merbit_spmv, C.c_int, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, i32, C.POINTER(C.c_float))
         _sig(L.ref_hll_sampled, C.c_int, vp, i32, i32, i32, u32, i32, i32, i32, vp, vp, vp)
@@ -212,3 +213,9 @@ def ref_get_width(nrow: int, nnz: int) -> int:
 def ref_predict(r) -> float:
     rr = np.ascontiguousarray(r, np.float64)
     return ref().ref_predict(_p(rr))
+
+
+def ref_local_swap(n: int, rho: float, near: int, window: int, seed: int) -> np.ndarray:
+    p = np.arange(n, dtype=np.int32)
+    ref().ref_local_swap(n, rho, near, window, seed, _p(p))
+    return p

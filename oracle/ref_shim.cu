@@ -63,6 +63,12 @@ void ref_pgorder_host(int nrow, const int* off1, const int* ind1, const int* off
     for (auto& f : futures) f.get();
 }
 
+/* local_swap (src/class.cu:236-301) on an identity-initialised permutation. */
+void ref_local_swap(int nrow, float rho, int near_, int window, unsigned long long seed, int* permutation)
+{
+    local_swap(nrow, rho, near_, window, seed, permutation);
+}
+
 double ref_predict(const double* r10)
 {
     std::array<double, rd_merbit_model::kFeatureCount> a{};
