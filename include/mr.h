@@ -116,6 +116,48 @@ int mr_merbit_plan_get_info(const mr_merbit_plan* plan, mr_merbit_plan_info* inf
  * output buffer (the reference's d_z) is needed. */
 int mr_spmv_merbit(const mr_merbit_plan* plan, const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
 
+/* ------------------------------------------------ batched SpMV ---- */
+
+/* Many independent y_i = A_i x_i in one persistent launch per (sigma,
+ * dtype) group, optionally replayed as a CUDA graph. No reference
+ * counterpart: the reference runs one matrix per process; this is the
+ * batched form of merbit_kernel (include/merbit.cuh:408-493). Each item's
+ * result is bitwise identical to mr_spmv_merbit on that item alone. */
+typedef struct mr_batch mr_batch;
+typedef struct mr_batch_item {
+    const mr_merbit_plan* plan;  /* plan of A (one plan may serve several items) */
+    mr_csr_view A;               /* the matrix the plan was built for */
+    const float* x;              /* device */
+    float* y;                    /* device */
+} mr_batch_item;
+
+int mr_batch_create(const mr_batch_item* items, int32_t count, void* stream, mr_batch** batch);
+int mr_batch_run(mr_batch* batch, void* stream);
+/* Captures mr_batch_run into a CUDA graph owned by the batch (stream must
+ * not be the legacy default stream); mr_batch_launch then replays it. */
+int mr_batch_capture(mr_batch* batch, void* stream);
+int mr_batch_launch(mr_batch* batch, void* stream);
+/* Points item i at new x / y; a captured graph stays valid. Synchronises
+ * `stream`. */
+int mr_batch_set_vectors(mr_batch* batch, int32_t i, const float* x, float* y, void* stream);
+int mr_batch_info(const mr_batch* batch, int32_t* groups, int64_t* total_tiles);
+int mr_batch_destroy(mr_batch* batch);
+
+/* Autotuner over MERBIT's tile size (sigma: items per lane, the tile is
+ * 32 x sigma merge items) and threads per CTA (block): times every supported
+ * pair on A (median of reps) and returns the fastest. The reference
+ * hard-codes BLOCK 256, SIGMA 14 (src/class.cu:1409-1410). */
+int mr_autotune_merbit(const mr_csr_view* A, const float* x_dev, float* y_dev, int32_t reps, int32_t* best_sigma,
+                       int32_t* best_block, float* best_ms, void* stream);
+/* Size-bucketed cache of tuning results: bucket = (floor(log2 rows),
+ * floor(log2 mean row length)); a miss tunes on the given matrix. */
+typedef struct mr_tuner mr_tuner;
+int mr_tuner_create(mr_tuner** tuner);
+int mr_tuner_destroy(mr_tuner* tuner);
+int mr_tuner_pick(mr_tuner* tuner, const mr_csr_view* A, const float* x_dev, float* y_dev, int32_t* sigma,
+                  int32_t* block, void* stream);
+int mr_tuner_stats(mr_tuner* tuner, int32_t* buckets, int32_t* tuned);
+
 /* ------------------------------------------------------ permutation ---- */
 
 /* B = P A P^T: B[perm[r], perm[c]] = A[r, c], columns sorted within rows,

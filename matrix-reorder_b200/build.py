@@ -33,7 +33,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-ffp-contract=o
 CU_SOURCES = ["abi.cu", "merbit.cu", "csr.cu", "permute.cu", "rd_exact.cu", "rd_hll.cu", "graph.cu",
               "batch.cu", "serve.cu"]
 CXX_SOURCES = ["pgorder.cpp", "predictor.cpp"]
-HEADERS = ["common.cuh", "internal.hpp"]
+HEADERS = ["common.cuh", "internal.hpp", "merbit_tile.cuh"]
 
 LIBMR = os.path.join(HERE, "libmr.so")
 LIBGEN = os.path.join(HERE, "libmr_gen.so")

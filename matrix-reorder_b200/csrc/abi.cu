@@ -36,9 +36,6 @@ static int check_view(const mr_csr_view* A, bool need_square)
 
 using namespace mr;
 
-struct mr_merbit_plan {
-    MerbitPlan p;
-};
 
 extern "C" {
 

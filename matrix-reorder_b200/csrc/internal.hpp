@@ -87,4 +87,9 @@ struct DevBuf {
 
 }  // namespace mr
 
+// opaque handle of include/mr.h
+struct mr_merbit_plan {
+    mr::MerbitPlan p;
+};
+
 #endif

@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "internal.hpp"
+#include "merbit_tile.cuh"
 
 namespace mr {
 
@@ -141,166 +142,21 @@ int launch_merbit_plan(const int* rowptr, int nrow, int nnz, int sigma, int lane
 
 // ----------------------------------------------------------------- SpMV ----
 
-template <int SIGMA> struct DescOf {
-    using T = typename std::conditional<(SIGMA < 15), uint32_t, unsigned long long>::type;
-    static constexpr int sh_flag = SIGMA < 15 ? 18 : 22;
-    static constexpr int sh_dy = SIGMA < 15 ? 9 : 11;
-    static constexpr unsigned mask_d = SIGMA < 15 ? 0x1ffu : 0x7ffu;
-};
-
-// Shared-memory words per warp: products of one tile (<= 32*SIGMA), shifted
-// by up to 3 so that 16-byte vectors stay aligned, plus slack.
-template <int SIGMA> constexpr int tile_smem_words() { return 32 * SIGMA + 8; }
-
 template <typename V, int SIGMA, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
-    merbit_spmv_kernel(const uint32_t* __restrict__ tile_x, const uint32_t* __restrict__ tile_y,
-                       const typename DescOf<SIGMA>::T* __restrict__ lane_desc, int tile_num, int lane_num,
-                       int64_t items, const int* __restrict__ colidx, const V* __restrict__ vals, int nnz,
-                       const float* __restrict__ x, float* __restrict__ y, float* __restrict__ carry, int vec_ok)
+__global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOperand<V, SIGMA> m, int tile_num)
 {
-    using D = DescOf<SIGMA>;
-    using DT = typename D::T;
-    constexpr int TW = tile_smem_words<SIGMA>();
-    __shared__ __align__(16) float s_buf[WARPS][TW];
-
-    const int warp = threadIdx.x >> 5, lid = threadIdx.x & 31;
+    __shared__ __align__(16) float s_buf[WARPS][tile_smem_words<SIGMA>()];
+    const int warp = threadIdx.x >> 5;
     const int tile = blockIdx.x * WARPS + warp;
     if (tile >= tile_num) return;
-    float* s = s_buf[warp];
-    const uint64_t pol = l2_evict_last_policy();
-
-    const int x0 = (int)__ldg(tile_x + tile);
-    const int x1 = (int)__ldg(tile_x + tile + 1);
-    const uint32_t ty0 = __ldg(tile_y + tile);
-    const int y0 = (int)(ty0 & 0x7fffffffu);
-    const int y1 = (int)(__ldg(tile_y + tile + 1) & 0x7fffffffu);
-    const bool single_row = (ty0 >> 31) != 0;
-
-    // ---- stage products vals[k] * x[colidx[k]] for k in [x0, x1) ---------
-    const int a0 = x0 & ~3;           // 16-byte aligned start
-    const int shift = x0 - a0;        // products of x0 land at s[shift]
-    const int nvec = (x1 - a0 + 3) >> 2;
-    float part = 0.f;                 // single-row tiles: running dot product
-    for (int v = lid; v < nvec; v += 32) {
-        const int k = a0 + 4 * v;
-        float p[4];
-        if (vec_ok && k + 3 < nnz) {
-            const int4 c = ld_stream(reinterpret_cast<const int4*>(colidx + k));
-            float w[4];
-            Vec4<V>::unpack(ld_stream(reinterpret_cast<const typename Vec4<V>::T*>(vals + k)), w);
-            const int cc[4] = {c.x, c.y, c.z, c.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) p[j] = (k + j >= x0 && k + j < x1) ? w[j] * ld_x(x + cc[j], pol) : 0.f;
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int kk = k + j;
-                p[j] = (kk >= x0 && kk < x1)
-                           ? ValueTraits<V>::f(ld_stream(vals + kk)) * ld_x(x + ld_stream(colidx + kk), pol)
-                           : 0.f;
-            }
-        }
-        if (single_row) {
-            part += (p[0] + p[1]) + (p[2] + p[3]);
-        } else {
-            *reinterpret_cast<float4*>(s + 4 * v) = make_float4(p[0], p[1], p[2], p[3]);
-        }
-    }
-    if (single_row) {
-        // every item of this tile is a nonzero of row y0 (== y1): the whole
-        // tile is a carry into that row
-        part = warp_sum(part);
-        if (lid == 0) carry[tile] = part;
-        return;
-    }
-    __syncwarp();
-
-    // ---- walk this lane's SIGMA merge items -------------------------------
-    const int gid = tile * 32 + lid;
-    int lane_items = 0;
-    DT d = 0;
-    if (gid < lane_num) {
-        lane_items = (int)min64((int64_t)SIGMA, items - (int64_t)gid * SIGMA);
-        d = __ldg(lane_desc + gid);
-    }
-    const uint32_t flags = (uint32_t)(d >> D::sh_flag) & ((lane_items >= 32) ? 0xffffffffu : ((1u << lane_items) - 1u));
-    int xi = shift + (int)(d & D::mask_d);
-    const int dy = (int)((d >> D::sh_dy) & D::mask_d);
-
-    float rows[SIGMA];  // finished row sums, indexed by the item that ends them
-    float cur = 0.f, head = 0.f;
-#pragma unroll
-    for (int i = 0; i < SIGMA; ++i) {
-        rows[i] = 0.f;
-        if (i < lane_items) {
-            if ((flags >> i) & 1u) {
-                rows[i] = cur;
-                cur = 0.f;
-            } else {
-                cur += s[xi];
-                ++xi;
-            }
-        }
-    }
-    const int nflags = __popc(flags);
-    const int first = nflags ? (__ffs(flags) - 1) : SIGMA;
-#pragma unroll
-    for (int i = 0; i < SIGMA; ++i)
-        if (i == first) head = rows[i];
-
-    // ---- warp segmented scan of the carried partial sums ------------------
-    // value: what this lane passes on (sum after its last row end); a lane
-    // with a row end starts a new segment.
-    float incl = cur;
-    bool seg = nflags != 0;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const float nv = __shfl_up_sync(0xffffffffu, incl, o);
-        const bool ns = __shfl_up_sync(0xffffffffu, seg, o);
-        if (lid >= o && !seg) {
-            incl += nv;
-            seg = ns;
-        }
-    }
-    float carry_in = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lid == 0) carry_in = 0.f;
-    const float tile_carry = __shfl_sync(0xffffffffu, incl, 31);
-    head += carry_in;
-    __syncwarp();  // all lanes are done reading products
-
-    // ---- finished rows -> shared -> coalesced stores ----------------------
-    int r = dy;
-#pragma unroll
-    for (int i = 0; i < SIGMA; ++i) {
-        if ((flags >> i) & 1u) {
-            s[r] = (i == first) ? head : rows[i];
-            ++r;
-        }
-    }
-    __syncwarp();
-    const int nrows = y1 - y0;
-    for (int j = lid; j < nrows; j += 32) __stcs(y + y0 + j, s[j]);
-    if (lid == 0) carry[tile] = tile_carry;
+    merbit_tile<V, SIGMA>(m, tile, s_buf[warp], l2_evict_last_policy());
 }
 
-// One thread per run of consecutive tiles whose open row at the tile end is
-// the same row R: y[R] += sum of their carries, summed in FP64 in tile order.
 __global__ void merbit_fixup_kernel(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
                                     int tile_num, int nrow, float* __restrict__ y)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= tile_num) return;
-    const int R = (int)(__ldg(tile_y + t + 1) & 0x7fffffffu);
-    if (R >= nrow) return;
-    if (t > 0 && (int)(__ldg(tile_y + t) & 0x7fffffffu) == R) return;  // not the first tile of the run
-    double s = 0.0;
-    int u = t;
-    do {
-        s += (double)carry[u];
-        ++u;
-    } while (u < tile_num && (int)(__ldg(tile_y + u + 1) & 0x7fffffffu) == R);
-    y[R] = (float)((double)y[R] + s);
+    if (t < tile_num) merbit_fixup_tile(tile_y, carry, tile_num, nrow, y, t);
 }
 
 template <typename V, int SIGMA, int WARPS>
@@ -310,11 +166,20 @@ static int launch_spmv_t(const MerbitPlan& p, const int* colidx, const void* val
     const int grid = (p.tile_num + WARPS - 1) / WARPS;
     const int vec_ok = ((reinterpret_cast<uintptr_t>(colidx) & 15) == 0) &&
                        ((reinterpret_cast<uintptr_t>(vals) & (4 * sizeof(V) - 1)) == 0);
-    if (grid > 0)
-        merbit_spmv_kernel<V, SIGMA, WARPS><<<grid, WARPS * 32, 0, st>>>(
-            p.tile_x, p.tile_y, reinterpret_cast<const typename DescOf<SIGMA>::T*>(p.lane_desc), p.tile_num,
-            p.lane_num, (int64_t)p.n_rows + p.nnz, colidx, reinterpret_cast<const V*>(vals), nnz, x, y, carry,
-            vec_ok);
+    MerbitOperand<V, SIGMA> m;
+    m.tile_x = p.tile_x;
+    m.tile_y = p.tile_y;
+    m.lane_desc = reinterpret_cast<const typename DescOf<SIGMA>::T*>(p.lane_desc);
+    m.lane_num = p.lane_num;
+    m.nnz = nnz;
+    m.items = (int64_t)p.n_rows + p.nnz;
+    m.colidx = colidx;
+    m.vals = reinterpret_cast<const V*>(vals);
+    m.x = x;
+    m.y = y;
+    m.carry = carry;
+    m.vec_ok = vec_ok;
+    if (grid > 0) merbit_spmv_kernel<V, SIGMA, WARPS><<<grid, WARPS * 32, 0, st>>>(m, p.tile_num);
     MR_CUDA_TRY(cudaGetLastError());
     if (p.tile_num > 0) {
         merbit_fixup_kernel<<<(p.tile_num + 255) / 256, 256, 0, st>>>(p.tile_y, carry, p.tile_num, p.n_rows, y);

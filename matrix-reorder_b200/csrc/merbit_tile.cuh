@@ -1,0 +1,222 @@
+// One MERBIT tile (32 lanes x SIGMA merge items) processed by one warp.
+// Shared by the single-matrix kernel (merbit.cu) and the batched persistent
+// kernel (batch.cu).
+//
+// Plan format (the reference's, include/merbit.cuh:84-131): lane descriptor
+// = flags << (18|22) | delta_row << (9|11) | delta_nz; tile_x = first nonzero
+// of the tile, tile_y = first row, bit 31 = all items are nonzeros of one row.
+//
+// Per tile: (1) every independent load is issued up front (tile bounds, the
+// lane's descriptor); (2) colidx/values of the tile are streamed as 16-byte
+// evict-first vectors, all vector loads of a round before any dependent x
+// gather, x gathered with an L2 evict-last policy, products staged in shared
+// memory; (3) each lane walks its SIGMA items from its descriptor, finished
+// rows stay in registers; (4) a warp segmented scan carries the partial sum
+// of a row across lanes; (5) finished rows leave through shared memory as
+// coalesced streaming stores, and the sum still open at the tile end goes to
+// carry[tile] for the FP64 fix-up. No atomics anywhere.
+#ifndef MR_MERBIT_TILE_CUH
+#define MR_MERBIT_TILE_CUH
+
+#include <type_traits>
+
+#include "common.cuh"
+
+namespace mr {
+
+template <int SIGMA> struct DescOf {
+    using T = typename std::conditional<(SIGMA < 15), uint32_t, unsigned long long>::type;
+    static constexpr int sh_flag = SIGMA < 15 ? 18 : 22;
+    static constexpr int sh_dy = SIGMA < 15 ? 9 : 11;
+    static constexpr unsigned mask_d = SIGMA < 15 ? 0x1ffu : 0x7ffu;
+};
+
+// Shared-memory words per warp: products of one tile (<= 32*SIGMA), shifted
+// by up to 3 so that 16-byte vectors stay aligned, plus slack.
+template <int SIGMA> constexpr int tile_smem_words() { return 32 * SIGMA + 8; }
+
+template <typename V, int SIGMA> struct MerbitOperand {
+    const uint32_t* tile_x;
+    const uint32_t* tile_y;
+    const typename DescOf<SIGMA>::T* lane_desc;
+    int lane_num;
+    int nnz;
+    int64_t items;  // n_rows + nnz
+    const int* colidx;
+    const V* vals;
+    const float* x;
+    float* y;
+    float* carry;
+    int vec_ok;     // colidx/vals aligned for vector loads
+};
+
+template <typename V, int SIGMA>
+__device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, const int tile, float* __restrict__ s,
+                                            const uint64_t pol)
+{
+    using D = DescOf<SIGMA>;
+    using DT = typename D::T;
+    const int lid = threadIdx.x & 31;
+    const int gid = tile * 32 + lid;
+
+    // ---- independent loads first ------------------------------------------
+    const int x0 = (int)__ldg(m.tile_x + tile);
+    const int x1 = (int)__ldg(m.tile_x + tile + 1);
+    const uint32_t ty0 = __ldg(m.tile_y + tile);
+    const int y1 = (int)(__ldg(m.tile_y + tile + 1) & 0x7fffffffu);
+    DT d = 0;
+    if (gid < m.lane_num) d = ld_stream(m.lane_desc + gid);
+    const int y0 = (int)(ty0 & 0x7fffffffu);
+    const bool single_row = (ty0 >> 31) != 0;
+
+    // ---- stage products vals[k] * x[colidx[k]] for k in [x0, x1) ---------
+    constexpr int NV = 8 * SIGMA + 1;  // max 4-element vectors per tile
+    constexpr int ITERS = (NV + 31) / 32;
+    constexpr int UNR = ITERS < 4 ? ITERS : 4;
+    const int a0 = x0 & ~3;  // 16-byte aligned start (FP32 / int32)
+    const int shift = x0 - a0;
+    const int nvec = (x1 - a0 + 3) >> 2;
+    float part = 0.f;
+#pragma unroll 1
+    for (int base = 0; base < ITERS; base += UNR) {
+        int col[UNR][4];
+        float val[UNR][4];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int v = lid + 32 * (base + u);
+            const int k = a0 + 4 * v;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                col[u][j] = 0;
+                val[u][j] = 0.f;
+            }
+            if (v < nvec) {
+                if (m.vec_ok && k + 3 < m.nnz) {
+                    const int4 c = ld_stream(reinterpret_cast<const int4*>(m.colidx + k));
+                    col[u][0] = c.x;
+                    col[u][1] = c.y;
+                    col[u][2] = c.z;
+                    col[u][3] = c.w;
+                    Vec4<V>::unpack(ld_stream(reinterpret_cast<const typename Vec4<V>::T*>(m.vals + k)), val[u]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int kk = k + j;
+                        if (kk >= x0 && kk < x1) {
+                            col[u][j] = ld_stream(m.colidx + kk);
+                            val[u][j] = ValueTraits<V>::f(ld_stream(m.vals + kk));
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            const int v = lid + 32 * (base + u);
+            if (v < nvec) {
+                const int k = a0 + 4 * v;
+                float p[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    p[j] = (k + j >= x0 && k + j < x1) ? val[u][j] * ld_x(m.x + col[u][j], pol) : 0.f;
+                if (single_row)
+                    part += (p[0] + p[1]) + (p[2] + p[3]);
+                else
+                    *reinterpret_cast<float4*>(s + 4 * v) = make_float4(p[0], p[1], p[2], p[3]);
+            }
+        }
+    }
+    if (single_row) {
+        // every item of this tile is a nonzero of row y0 (== y1): the whole
+        // tile is a carry into that row
+        part = warp_sum(part);
+        if (lid == 0) m.carry[tile] = part;
+        return;
+    }
+    __syncwarp();
+
+    // ---- walk this lane's SIGMA merge items -------------------------------
+    const int lane_items = gid < m.lane_num ? (int)min64((int64_t)SIGMA, m.items - (int64_t)gid * SIGMA) : 0;
+    const uint32_t flags =
+        (uint32_t)(d >> D::sh_flag) & ((lane_items >= 32) ? 0xffffffffu : ((1u << lane_items) - 1u));
+    int xi = shift + (int)(d & D::mask_d);
+    const int dy = (int)((d >> D::sh_dy) & D::mask_d);
+
+    float rows[SIGMA];  // finished row sums, indexed by the item that ends them
+    float cur = 0.f;
+#pragma unroll
+    for (int i = 0; i < SIGMA; ++i) {
+        rows[i] = 0.f;
+        if (i < lane_items) {
+            if ((flags >> i) & 1u) {
+                rows[i] = cur;
+                cur = 0.f;
+            } else {
+                cur += s[xi];
+                ++xi;
+            }
+        }
+    }
+    const int first = flags ? (__ffs(flags) - 1) : SIGMA;
+    float head = 0.f;
+#pragma unroll
+    for (int i = 0; i < SIGMA; ++i)
+        if (i == first) head = rows[i];
+
+    // ---- warp segmented scan of the carried partial sums ------------------
+    // a lane passes on its sum after its last row end; a lane with a row end
+    // starts a new segment
+    float incl = cur;
+    bool seg = flags != 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float nv = __shfl_up_sync(0xffffffffu, incl, o);
+        const bool ns = __shfl_up_sync(0xffffffffu, seg, o);
+        if (lid >= o && !seg) {
+            incl += nv;
+            seg = ns;
+        }
+    }
+    float carry_in = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lid == 0) carry_in = 0.f;
+    const float tile_carry = __shfl_sync(0xffffffffu, incl, 31);
+    head += carry_in;
+    __syncwarp();  // all lanes are done reading products
+
+    // ---- finished rows -> shared -> coalesced stores ----------------------
+    int r = dy;
+#pragma unroll
+    for (int i = 0; i < SIGMA; ++i) {
+        if ((flags >> i) & 1u) {
+            s[r] = (i == first) ? head : rows[i];
+            ++r;
+        }
+    }
+    __syncwarp();
+    const int nrows = y1 - y0;
+    for (int j = lid; j < nrows; j += 32) __stcs(m.y + y0 + j, s[j]);
+    if (lid == 0) m.carry[tile] = tile_carry;
+    __syncwarp();  // the warp may reuse s for its next tile
+}
+
+// Adds each run of carries to its row: the thread of the first tile of a run
+// of tiles whose open row at the tile end is the same row R sums their
+// carries in FP64, in tile order, and finishes y[R].
+__device__ __forceinline__ void merbit_fixup_tile(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
+                                                  int tile_num, int nrow, float* __restrict__ y, int t)
+{
+    const int R = (int)(__ldg(tile_y + t + 1) & 0x7fffffffu);
+    if (R >= nrow) return;
+    if (t > 0 && (int)(__ldg(tile_y + t) & 0x7fffffffu) == R) return;  // not the first tile of the run
+    double acc = 0.0;
+    int u = t;
+    do {
+        acc += (double)carry[u];
+        ++u;
+    } while (u < tile_num && (int)(__ldg(tile_y + u + 1) & 0x7fffffffu) == R);
+    y[R] = (float)((double)y[R] + acc);
+}
+
+}  // namespace mr
+
+#endif

@@ -436,3 +436,114 @@ def random_perm(n: int, seed: int) -> np.ndarray:
     out = np.empty(n, np.int32)
     gen().mrg_random_perm(n, seed, out.ctypes.data)
     return out
+
+
+# --------------------------------------------------------------- batching ----
+
+class BatchItem(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("A", CsrView), ("x", C.c_void_p), ("y", C.c_void_p)]
+
+
+def _batch_sigs(L):
+    if getattr(L, "_batch_sigs", False):
+        return
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    P = C.POINTER
+    _sig(L.mr_batch_create, C.c_int, P(BatchItem), i32, vp, P(vp))
+    _sig(L.mr_batch_run, C.c_int, vp, vp)
+    _sig(L.mr_batch_capture, C.c_int, vp, vp)
+    _sig(L.mr_batch_launch, C.c_int, vp, vp)
+    _sig(L.mr_batch_set_vectors, C.c_int, vp, i32, vp, vp, vp)
+    _sig(L.mr_batch_info, C.c_int, vp, P(i32), P(i64))
+    _sig(L.mr_batch_destroy, C.c_int, vp)
+    _sig(L.mr_autotune_merbit, C.c_int, P(CsrView), vp, vp, i32, P(i32), P(i32), P(C.c_float), vp)
+    _sig(L.mr_tuner_create, C.c_int, P(vp))
+    _sig(L.mr_tuner_destroy, C.c_int, vp)
+    _sig(L.mr_tuner_pick, C.c_int, vp, P(CsrView), vp, vp, P(i32), P(i32), vp)
+    _sig(L.mr_tuner_stats, C.c_int, vp, P(i32), P(i32))
+    L._batch_sigs = True
+
+
+class Batch:
+    """mr_batch over (MerbitPlan, x, y) triples; keeps its operands alive."""
+
+    def __init__(self, entries, stream=None):
+        L = lib()
+        _batch_sigs(L)
+        self.entries = list(entries)
+        arr = (BatchItem * len(self.entries))()
+        for i, (plan, x, y) in enumerate(self.entries):
+            arr[i] = BatchItem(plan.h.value, plan.A, _ptr(x), _ptr(y))
+        h = C.c_void_p()
+        check(L.mr_batch_create(arr, len(self.entries), _stream(stream), C.byref(h)), "mr_batch_create")
+        self.h = h
+
+    def run(self, stream=None):
+        check(lib().mr_batch_run(self.h, _stream(stream)), "mr_batch_run")
+
+    def capture(self, stream):
+        check(lib().mr_batch_capture(self.h, _stream(stream)), "mr_batch_capture")
+
+    def launch(self, stream=None):
+        check(lib().mr_batch_launch(self.h, _stream(stream)), "mr_batch_launch")
+
+    def set_vectors(self, i, x, y, stream=None):
+        plan = self.entries[i][0]
+        self.entries[i] = (plan, x, y)
+        check(lib().mr_batch_set_vectors(self.h, i, _ptr(x), _ptr(y), _stream(stream)), "mr_batch_set_vectors")
+
+    def info(self):
+        g, t = C.c_int32(0), C.c_int64(0)
+        check(lib().mr_batch_info(self.h, C.byref(g), C.byref(t)), "mr_batch_info")
+        return g.value, t.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(A: CsrView, x, y, reps: int = 5, stream=None):
+    L = lib()
+    _batch_sigs(L)
+    s, b, ms = C.c_int32(0), C.c_int32(0), C.c_float(0)
+    check(L.mr_autotune_merbit(C.byref(A), _ptr(x), _ptr(y), reps, C.byref(s), C.byref(b), C.byref(ms),
+                               _stream(stream)), "mr_autotune_merbit")
+    return s.value, b.value, ms.value
+
+
+class Tuner:
+    def __init__(self):
+        L = lib()
+        _batch_sigs(L)
+        h = C.c_void_p()
+        check(L.mr_tuner_create(C.byref(h)), "mr_tuner_create")
+        self.h = h
+
+    def pick(self, A: CsrView, x, y, stream=None):
+        s, b = C.c_int32(0), C.c_int32(0)
+        check(lib().mr_tuner_pick(self.h, C.byref(A), _ptr(x), _ptr(y), C.byref(s), C.byref(b), _stream(stream)),
+              "mr_tuner_pick")
+        return s.value, b.value
+
+    def stats(self):
+        a, b = C.c_int32(0), C.c_int32(0)
+        check(lib().mr_tuner_stats(self.h, C.byref(a), C.byref(b)), "mr_tuner_stats")
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mr_tuner_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -171,6 +171,10 @@ int ref_gorder4_full(int nrow, int nnz, int* d_row_ind, int* d_col_ind, float* d
                      int* h_perm_out)
 {
     ENV env(0, "", "");
+    // ENV always selects device 1 (include/class.cuh:23); on a one-GPU box
+    // that fails and leaves an error that Thrust would report later
+    cudaSetDevice(0);
+    cudaGetLastError();
     GRAPH<float> g;
     g.nrow = nrow;
     g.nnz = nnz;
