@@ -379,7 +379,7 @@ def main() -> int:
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--sigma", type=int, default=14)
-    ap.add_argument("--block", type=int, default=256)
+    ap.add_argument("--block", type=int, default=1024)
     ap.add_argument("--e2e-steps", type=int, default=400)
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of CPU-baseline timing")
     ap.add_argument("--quick", action="store_true", help="skip companion numbers and CPU baseline")

@@ -74,9 +74,9 @@ int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stre
     *out = nullptr;
     MR_TRY(check_view(A, false));
     if (sigma == 0) sigma = 14;
-    if (block == 0) block = 256;
+    if (block == 0) block = 1024;
     if (sigma < 1 || sigma > 42) return MR_ERR_INVALID_ARG;
-    if (block != 128 && block != 256 && block != 512) return MR_ERR_UNSUPPORTED;
+    if (block != 128 && block != 256 && block != 512 && block != 1024) return MR_ERR_UNSUPPORTED;
     const int64_t items = (int64_t)A->n_rows + A->nnz;
     if (items + 32ll * sigma * 257 > (int64_t)INT32_MAX) return MR_ERR_INVALID_ARG;
     {
@@ -101,16 +101,19 @@ int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stre
         cudaFree(p.tile_y);
         cudaFree(p.lane_desc);
         cudaFree(p.carry);
+        cudaFree(p.ticket);
         delete h;
         return code;
     };
     if (cudaMalloc(&p.tile_x, sizeof(uint32_t) * ((size_t)p.tile_num + 1)) != cudaSuccess ||
         cudaMalloc(&p.tile_y, sizeof(uint32_t) * ((size_t)p.tile_num + 1)) != cudaSuccess ||
         cudaMalloc(&p.lane_desc, desc_bytes * (size_t)std::max(p.lane_num, 1)) != cudaSuccess ||
-        cudaMalloc(&p.carry, sizeof(float) * (size_t)std::max(p.tile_num, 1)) != cudaSuccess) {
+        cudaMalloc(&p.carry, sizeof(float) * (size_t)std::max(p.tile_num, 1)) != cudaSuccess ||
+        cudaMalloc(&p.ticket, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         return fail(MR_ERR_NOMEM);
     }
+    if (cudaMemsetAsync(p.ticket, 0, sizeof(int), st) != cudaSuccess) return fail(MR_ERR_CUDA);
     int s = launch_merbit_plan(A->rowptr, A->n_rows, (int)A->nnz, sigma, p.lane_num, p.tile_num, p.tile_x, p.tile_y,
                                p.lane_desc, st);
     if (s != MR_OK) return fail(s);
@@ -129,6 +132,7 @@ int mr_merbit_plan_destroy(mr_merbit_plan* h)
     cudaFree(h->p.tile_y);
     cudaFree(h->p.lane_desc);
     cudaFree(h->p.carry);
+    cudaFree(h->p.ticket);
     if (dev != h->p.device) cudaSetDevice(dev);
     delete h;
     return MR_OK;

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(WARPS * 32)
 {
     __shared__ __align__(16) float s_buf[WARPS][tile_smem_words<SIGMA>()];
     const int warp = threadIdx.x >> 5;
-    const uint64_t pol = l2_evict_last_policy();
+    const TilePolicy pol{l2_evict_last_policy(), 0};
     const long long stride = (long long)gridDim.x * WARPS;
     for (long long g = (long long)blockIdx.x * WARPS + warp; g < total_tiles; g += stride) {
         const int it = find_item(prefix, count, g);
@@ -381,7 +381,7 @@ int mr_autotune_merbit(const mr_csr_view* A, const float* x, float* y, int32_t r
 {
     if (!A || !best_sigma || !best_block) return MR_ERR_INVALID_ARG;
     static const int sigmas[] = {7, 10, 14, 16, 20, 24, 28, 32};
-    static const int blocks[] = {128, 256, 512};
+    static const int blocks[] = {128, 256, 512, 1024};
     if (reps < 1) reps = 5;
     cudaStream_t st = as_stream(stream);
     cudaEvent_t e0, e1;
@@ -392,7 +392,7 @@ int mr_autotune_merbit(const mr_csr_view* A, const float* x, float* y, int32_t r
     int status = MR_OK;
     for (int s : sigmas) {
         mr_merbit_plan* plan = nullptr;
-        status = mr_merbit_plan_create(A, s, 256, stream, &plan);
+        status = mr_merbit_plan_create(A, s, 1024, stream, &plan);
         if (status != MR_OK) break;
         for (int blk : blocks) {
             plan->p.block = blk;
@@ -475,7 +475,7 @@ int mr_tuner_pick(mr_tuner* t, const mr_csr_view* A, const float* x, float* y, i
             return MR_OK;
         }
     }
-    int s = 14, b = 256;
+    int s = 14, b = 1024;
     MR_TRY(mr_autotune_merbit(A, x, y, 5, &s, &b, nullptr, stream));
     std::lock_guard<std::mutex> lk(t->mu);
     t->best[key] = {s, b};

@@ -111,6 +111,51 @@ __device__ __forceinline__ __nv_bfloat16 ld_stream(const __nv_bfloat16* p)
     return __ushort_as_bfloat16(u);
 }
 
+// Streams that the persistent SpMV reads once: bypass L1 (so L1 holds only
+// x) and mark them evict-first in L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ int4 ld_na(const int4* p, uint64_t pol)
+{
+    int4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float4 ld_na(const float4* p, uint64_t pol)
+{
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ uint2 ld_na(const uint2* p, uint64_t pol)
+{
+    uint2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+                 : "=r"(v.x), "=r"(v.y)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ unsigned ld_na(const unsigned* p, uint64_t pol)
+{
+    unsigned v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_na(const unsigned long long* p, uint64_t pol)
+{
+    unsigned long long v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 // x is gathered many times per SpMV: keep it in L2 (evict-last policy) and
 // use the read-only path.
 __device__ __forceinline__ uint64_t l2_evict_last_policy()

@@ -209,7 +209,8 @@ int mr_graph_spmv(mr_graph* g, const char* method, int32_t iters, const float* x
     mr_merbit_plan* plan = nullptr;
     int s = MR_OK;
     cudaEventRecord(e0, g->st);
-    if (m == "merbit") s = mr_merbit_plan_create(&v, 14, 256, g->st, &plan);  // BLOCK 256, SIGMA 14 (src/class.cu:1409-1410)
+    // SIGMA 14 as the reference (src/class.cu:1409-1410); the B200 kernel picks its own CTA shape
+    if (m == "merbit") s = mr_merbit_plan_create(&v, 14, 0, g->st, &plan);
     cudaEventRecord(e1, g->st);
     for (int it = 0; it < iters && s == MR_OK; ++it)
         s = plan ? mr_spmv_merbit(plan, &v, xp.as<float>(), yp.as<float>(), g->st)

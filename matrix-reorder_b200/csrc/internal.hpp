@@ -22,6 +22,7 @@ struct MerbitPlan {
     uint32_t* tile_y = nullptr;   // tile_num + 1
     void* lane_desc = nullptr;    // lane_num words (4 or 8 bytes)
     float* carry = nullptr;       // tile_num carries
+    int* ticket = nullptr;        // persistent kernel's completion counter (starts at 0)
     int device = 0;
 };
 

@@ -22,6 +22,7 @@
 //    carry slot, and a second kernel adds each run of carries to its row in
 //    FP64 in tile order. Results are bitwise reproducible run to run.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -149,7 +150,84 @@ __global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOpe
     const int warp = threadIdx.x >> 5;
     const int tile = blockIdx.x * WARPS + warp;
     if (tile >= tile_num) return;
-    merbit_tile<V, SIGMA>(m, tile, s_buf[warp], l2_evict_last_policy());
+    merbit_tile<V, SIGMA>(m, tile, s_buf[warp], TilePolicy{l2_evict_last_policy(), 0});
+}
+
+// ---- persistent form: one CTA of 32 warps per SM sweeps a contiguous chunk
+// of tiles, so the warps resident on an SM work on neighbouring rows and the
+// reordered matrix's x reuse is caught by L1 (the streams bypass L1). Rows
+// whose carry run stays inside a chunk are finished by the chunk's CTA after
+// a barrier; the last CTA to finish (atomic ticket after a fence) finishes
+// the runs that cross chunk boundaries. Same FP64 run sums, same order, as
+// the two-kernel form: the results are bit-identical.
+constexpr int kPersistWarps = 32;
+
+__device__ __forceinline__ int open_row(const uint32_t* tile_y, int t)
+{
+    return (int)(__ldg(tile_y + t + 1) & 0x7fffffffu);
+}
+
+// run that starts in [t0, t1) and whose row ends inside the chunk
+__device__ __forceinline__ void fixup_in_chunk(const uint32_t* __restrict__ tile_y, const float* carry, int t0, int t1,
+                                               int nrow, float* y, int t)
+{
+    const int R = open_row(tile_y, t);
+    if (R >= nrow) return;
+    if (t > 0 && open_row(tile_y, t - 1) == R) return;  // not the first tile of its run
+    double acc = 0.0;
+    int u = t;
+    while (u < t1 && open_row(tile_y, u) == R) {
+        acc += (double)carry[u];
+        ++u;
+    }
+    if (u >= t1) return;  // the row ends in a later chunk: boundary pass
+    y[R] = (float)((double)y[R] + acc);
+}
+
+// run that crosses the boundary at the start of chunk c and whose row ends
+// inside chunk c (each crossing run is finished at exactly one boundary)
+__device__ __forceinline__ void fixup_boundary(const uint32_t* __restrict__ tile_y, const float* carry, int tile_num,
+                                               int chunk, int nrow, float* y, int c)
+{
+    const int b = c * chunk;
+    if (b <= 0 || b >= tile_num) return;
+    const int p = b - 1;
+    const int R = open_row(tile_y, p);
+    if (R >= nrow) return;
+    int ue = p;
+    while (ue + 1 < tile_num && open_row(tile_y, ue + 1) == R) ++ue;
+    if (ue + 1 >= min(b + chunk, tile_num)) return;  // ends beyond chunk c
+    int u0 = p;
+    while (u0 > 0 && open_row(tile_y, u0 - 1) == R) --u0;
+    double acc = 0.0;
+    for (int u = u0; u <= ue; ++u) acc += (double)__ldcg(carry + u);
+    y[R] = (float)((double)__ldcg(y + R) + acc);
+}
+
+template <typename V, int SIGMA>
+__global__ void __launch_bounds__(kPersistWarps * 32, 1)
+    merbit_persistent_kernel(const MerbitOperand<V, SIGMA> m, int tile_num, int nrow, int* __restrict__ ticket)
+{
+    extern __shared__ __align__(16) float s_dyn[];
+    __shared__ int s_last;
+    const int warp = threadIdx.x >> 5;
+    const int G = gridDim.x;
+    const int chunk = (tile_num + G - 1) / G;
+    const int t0 = min((int)blockIdx.x * chunk, tile_num);
+    const int t1 = min(t0 + chunk, tile_num);
+    float* s = s_dyn + warp * tile_smem_words<SIGMA>();
+    const TilePolicy pol{l2_evict_last_policy(), l2_evict_first_policy()};
+    for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true>(m, t, s, pol);
+    __syncthreads();
+    for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x) fixup_in_chunk(m.tile_y, m.carry, t0, t1, nrow, m.y, t);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1) == G - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int c = 1 + (int)threadIdx.x; c < G; c += blockDim.x) fixup_boundary(m.tile_y, m.carry, tile_num, chunk, nrow, m.y, c);
+    if (threadIdx.x == 0) *ticket = 0;  // ready for the next launch
 }
 
 __global__ void merbit_fixup_kernel(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
@@ -189,10 +267,48 @@ static int launch_spmv_t(const MerbitPlan& p, const int* colidx, const void* val
 }
 
 template <typename V, int SIGMA>
+static int launch_persistent(const MerbitPlan& p, const int* colidx, const void* vals, int nnz, const float* x,
+                             float* y, float* carry, cudaStream_t st)
+{
+    if (p.tile_num == 0) return MR_OK;
+    MerbitOperand<V, SIGMA> m;
+    m.tile_x = p.tile_x;
+    m.tile_y = p.tile_y;
+    m.lane_desc = reinterpret_cast<const typename DescOf<SIGMA>::T*>(p.lane_desc);
+    m.lane_num = p.lane_num;
+    m.nnz = nnz;
+    m.items = (int64_t)p.n_rows + p.nnz;
+    m.colidx = colidx;
+    m.vals = reinterpret_cast<const V*>(vals);
+    m.x = x;
+    m.y = y;
+    m.carry = carry;
+    m.vec_ok = ((reinterpret_cast<uintptr_t>(colidx) & 15) == 0) &&
+               ((reinterpret_cast<uintptr_t>(vals) & (4 * sizeof(V) - 1)) == 0);
+    const size_t smem = sizeof(float) * (size_t)kPersistWarps * tile_smem_words<SIGMA>();
+    static bool configured = false;  // per instantiation; attributes are per device but idempotent
+    if (!configured) {
+        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // smallest shared-memory carve-out that fits: the rest of the SM's
+        // 256 KB stays L1 for x
+        const int pct = (int)((smem + 1023) / 1024 * 100 / 228) + 1;
+        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA>,
+                                         cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100)));
+        configured = true;
+    }
+    const int grid = std::max(1, std::min(sm_count(), (p.tile_num + kPersistWarps - 1) / kPersistWarps));
+    merbit_persistent_kernel<V, SIGMA><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows, p.ticket);
+    MR_CUDA_TRY(cudaGetLastError());
+    return MR_OK;
+}
+
+template <typename V, int SIGMA>
 static int launch_spmv_w(const MerbitPlan& p, const int* colidx, const void* vals, int nnz, const float* x, float* y,
                          float* carry, cudaStream_t st)
 {
     switch (p.block) {
+    case 1024: return launch_persistent<V, SIGMA>(p, colidx, vals, nnz, x, y, carry, st);
     case 128: return launch_spmv_t<V, SIGMA, 4>(p, colidx, vals, nnz, x, y, carry, st);
     case 512:
         // 16 warps only while the static staging buffers fit in 48 KB

@@ -50,10 +50,27 @@ template <typename V, int SIGMA> struct MerbitOperand {
     int vec_ok;     // colidx/vals aligned for vector loads
 };
 
-template <typename V, int SIGMA>
-__device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, const int tile, float* __restrict__ s,
-                                            const uint64_t pol)
+// Cache policies of one tile: x gathers keep their lines in L2 (evict-last);
+// with NA the matrix streams bypass L1 and are evict-first in L2, so that
+// L1 caches only x.
+struct TilePolicy {
+    uint64_t x_keep;
+    uint64_t stream_first;
+};
+
+template <bool NA, typename T> __device__ __forceinline__ T ld_s(const T* p, uint64_t pol)
 {
+    if constexpr (NA)
+        return ld_na(p, pol);
+    else
+        return ld_stream(p);
+}
+
+template <typename V, int SIGMA, bool NA = false>
+__device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, const int tile, float* __restrict__ s,
+                                            const TilePolicy pols)
+{
+    const uint64_t pol = pols.x_keep;
     using D = DescOf<SIGMA>;
     using DT = typename D::T;
     const int lid = threadIdx.x & 31;
@@ -65,7 +82,7 @@ __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, co
     const uint32_t ty0 = __ldg(m.tile_y + tile);
     const int y1 = (int)(__ldg(m.tile_y + tile + 1) & 0x7fffffffu);
     DT d = 0;
-    if (gid < m.lane_num) d = ld_stream(m.lane_desc + gid);
+    if (gid < m.lane_num) d = ld_s<NA>(m.lane_desc + gid, pols.stream_first);
     const int y0 = (int)(ty0 & 0x7fffffffu);
     const bool single_row = (ty0 >> 31) != 0;
 
@@ -92,12 +109,13 @@ __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, co
             }
             if (v < nvec) {
                 if (m.vec_ok && k + 3 < m.nnz) {
-                    const int4 c = ld_stream(reinterpret_cast<const int4*>(m.colidx + k));
+                    const int4 c = ld_s<NA>(reinterpret_cast<const int4*>(m.colidx + k), pols.stream_first);
                     col[u][0] = c.x;
                     col[u][1] = c.y;
                     col[u][2] = c.z;
                     col[u][3] = c.w;
-                    Vec4<V>::unpack(ld_stream(reinterpret_cast<const typename Vec4<V>::T*>(m.vals + k)), val[u]);
+                    Vec4<V>::unpack(ld_s<NA>(reinterpret_cast<const typename Vec4<V>::T*>(m.vals + k), pols.stream_first),
+                                    val[u]);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {

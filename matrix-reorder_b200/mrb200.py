@@ -151,7 +151,7 @@ def spmv_csr(A: CsrView, x, y, stream=None) -> None:
 class MerbitPlan:
     """Owner of an mr_merbit_plan (the reference's TILE<BLOCK,SIGMA>)."""
 
-    def __init__(self, A: CsrView, sigma: int = 14, block: int = 256, stream=None):
+    def __init__(self, A: CsrView, sigma: int = 14, block: int = 0, stream=None):
         h = C.c_void_p()
         check(lib().mr_merbit_plan_create(C.byref(A), sigma, block, _stream(stream), C.byref(h)),
               "mr_merbit_plan_create")

@@ -24,7 +24,7 @@ def _rel_l2(got, ref):
     return d / nr if nr > 0 else d
 
 
-def _plan_and_spmv(M, rp, ci, v, x, sigma=14, block=256, dtype=None):
+def _plan_and_spmv(M, rp, ci, v, x, sigma=14, block=0, dtype=None):
     import torch
     vals = _dev(v)
     if dtype is not None:
@@ -113,13 +113,32 @@ def test_merbit_spmv_matches_fp64(M, O, cases, sigma):
         plan.close()
 
 
-@pytest.mark.parametrize("block", [128, 256, 512])
+@pytest.mark.parametrize("block", [128, 256, 512, 1024])
 def test_merbit_block_sizes(M, O, cases, block):
     rp, ci, v = cases["rmat13"]
     x = M.uniform(rp.size - 1, seed=5)
     plan, y, _ = _plan_and_spmv(M, rp, ci, v, x, block=block)
     assert _rel_l2(y, O.spmv_f64(rp, ci, v, x)) <= REL_L2_F32
     plan.close()
+
+
+@pytest.mark.parametrize("sigma", [7, 14, 32])
+def test_persistent_and_two_kernel_forms_bit_identical(M, cases, sigma):
+    """The persistent kernel finishes carry runs inside its chunk and at chunk
+    boundaries; the two-kernel form in one fix-up pass. Both sum each run in
+    FP64 in tile order, so they must agree bit for bit."""
+    import torch
+    rp, ci, v = M.gen_rmat(scale=17, edge_factor=16, seed=8)
+    big = dict(cases)
+    big["rmat17"] = (rp, ci, v)
+    for name, (rp, ci, v) in big.items():
+        ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+        x = M.uniform(ncols, seed=2)
+        p1, y1, _ = _plan_and_spmv(M, rp, ci, v, x, sigma=sigma, block=1024)
+        p2, y2, _ = _plan_and_spmv(M, rp, ci, v, x, sigma=sigma, block=256)
+        assert np.array_equal(y1.view(np.int32), y2.view(np.int32)), (name, sigma)
+        p1.close()
+        p2.close()
 
 
 def test_merbit_is_deterministic(M, cases):
