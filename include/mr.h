@@ -116,6 +116,22 @@ int mr_merbit_plan_get_info(const mr_merbit_plan* plan, mr_merbit_plan_info* inf
  * output buffer (the reference's d_z) is needed. */
 int mr_spmv_merbit(const mr_merbit_plan* plan, const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
 
+/* Allocation-free MERBIT SpMV: y = A x with no device allocation at all.
+ * No counterpart in the reference (which allocates its plan and buffers
+ * with cudaMalloc, include/merbit.cuh:146-151); it exists for callers that
+ * cannot call cudaMalloc while they run SpMV, e.g. code whose device memory
+ * is owned by another runtime's pool, or that must not synchronise the
+ * device by allocating. The plan (SIGMA 14), carries and completion ticket
+ * live in one file-scope device array sized for n_rows + nnz <= 2^24 merge
+ * items (about 5.3 MB that every GPU which loads the library keeps until
+ * exit); larger matrices return MR_ERR_UNSUPPORTED. The caller passes A, x
+ * and y as for mr_spmv_merbit; each call rebuilds the plan into the array
+ * and gives the same result as a planned call. The first call on a device
+ * looks up the array's device address: make it before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race:
+ * order them on one stream. */
+int mr_spmv_merbit_noalloc(const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
+
 /* ------------------------------------------------ batched SpMV ---- */
 
 /* Many independent y_i = A_i x_i in one persistent launch per (sigma,
