@@ -233,11 +233,19 @@ def run_ours(args):
     B = M.view(brp, bci, bv)
     xp = torch.empty_like(x_d)
     M.permute_vector(perm_d, x_d, xp, inverse=False)
+    yp = torch.empty_like(x_d)
+    hub_cache = True
+    if args.tune:
+        # the project's autotuner picks sigma (tile = 32 x sigma merge items),
+        # threads per CTA and the hub cache on this matrix (setup, untimed)
+        t0 = time.perf_counter()
+        args.sigma, args.block, flags, _ = M.autotune(B, xp, yp, reps=5)
+        hub_cache = (flags & 1) == 0
+        setup["autotune_s"] = round(time.perf_counter() - t0, 2)
     t0 = time.perf_counter()
-    plan = M.MerbitPlan(B, sigma=args.sigma, block=args.block)
+    plan = M.MerbitPlan(B, sigma=args.sigma, block=args.block, hub_cache=hub_cache)
     torch.cuda.synchronize()
     setup["plan_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
-    yp = torch.empty_like(x_d)
     bytes_step = spmv_bytes(n, nnz)
 
     def timed(fn, steps, warm):
@@ -261,6 +269,18 @@ def run_ours(args):
         plan_a = M.MerbitPlan(A, sigma=args.sigma, block=args.block)
         details["merbit_orig_gbs"] = round(bytes_step / timed(lambda: plan_a.spmv(x_d, yd), 50, 5) / 1e6, 1)
         plan_a.close()
+        plan_nh = M.MerbitPlan(B, sigma=args.sigma, block=args.block, hub_cache=False)
+        details["merbit_reordered_no_hub_cache_gbs"] = round(
+            bytes_step / timed(lambda: plan_nh.spmv(xp, yp), 50, 5) / 1e6, 1)
+        plan_nh.close()
+        # the reference's fixed configuration: SIGMA 14, 256 threads (src/class.cu:1409-1410)
+        plan_r = M.MerbitPlan(B, sigma=14, block=256, hub_cache=False)
+        details["merbit_reordered_sigma14_block256_gbs"] = round(
+            bytes_step / timed(lambda: plan_r.spmv(xp, yp), 50, 5) / 1e6, 1)
+        plan_r.close()
+    inf = plan.info()
+    details["hub_columns"] = inf.hub_columns
+    details["hub_coverage"] = round(inf.hub_coverage, 4)
 
     # ---- headline: K MERBIT SpMVs on the reordered matrix ----
     for _ in range(args.warmup):
@@ -333,7 +353,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_spmv": bytes_step,
-                "kernels_timed": "merbit_spmv_kernel + merbit_fixup_kernel (one SpMV)"}
+                "kernels_timed": "one MERBIT SpMV (persistent kernel with fused fix-up, or grid kernel + fix-up)"}
 
     cpu = None
     if rank == 0 and not args.quick and args.cpu_budget > 0:
@@ -351,6 +371,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"rmat_s{args.scale}_ef{args.edge_factor} pGOrder-reordered MERBIT FP32 SpMV",
                        "n_rows": n, "nnz": nnz, "seed": args.seed, "sigma": args.sigma, "block": args.block,
+                       "hub_cache": bool(hub_cache), "tuned": bool(args.tune),
                        "parallelism": f"replicas x{ws}",
                        "l2": "inputs larger than L2 (matrix stream ~%d MB per step)" % (bytes_step // 2**20)},
             "roofline": roofline,
@@ -383,6 +404,7 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=400)
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of CPU-baseline timing")
     ap.add_argument("--quick", action="store_true", help="skip companion numbers and CPU baseline")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="use --sigma/--block instead of the autotuner")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

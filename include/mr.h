@@ -84,9 +84,10 @@ int mr_spmv_csr(const mr_csr_view* A, const float* x_dev, float* y_dev, void* st
  * TILE<BLOCK,SIGMA>::TILE builds (include/merbit.cuh:134-155, Tile_Kernel
  * :55-131): tile_x/tile_y[tile_num+1] (bit 31 of tile_y = single-row tile)
  * and lane_desc[lane_num] (32-bit words for sigma < 15, 64-bit otherwise).
- * sigma: merge items per lane, 1..42 (reference 14). block: threads per CTA
- * of the SpMV kernel, a multiple of 32 in [32, 1024] (reference 256); 0
- * picks the default. The plan also owns the per-tile carry-out scratch.
+ * sigma: merge items per lane, 1..42 (reference 14; the SpMV kernels are
+ * built for 7, 10, 14, 16, 20, 24, 28, 32). block: threads per CTA of the
+ * SpMV kernel, 128, 256, 512 or 1024 (reference 256); 0 picks 1024. The
+ * plan also owns the per-tile carry-out scratch.
  * The rowptr of A must stay unchanged while the plan is used. */
 typedef struct mr_merbit_plan mr_merbit_plan;
 
@@ -101,9 +102,31 @@ typedef struct mr_merbit_plan_info {
     const uint32_t* tile_x_dev;   /* tile_num + 1 */
     const uint32_t* tile_y_dev;   /* tile_num + 1 */
     const void* lane_desc_dev;    /* lane_num words of desc_bytes */
+    int32_t hub_columns;          /* columns staged in shared memory (0: no hub cache) */
+    double hub_coverage;          /* share of nonzeros whose x comes from the hub cache */
 } mr_merbit_plan_info;
 
+/* block 1024 (the default) selects the persistent kernel: one CTA of 32
+ * warps per SM sweeping a contiguous range of tiles, with the carry fix-up
+ * fused in. Its plan also builds a hub cache when it pays: the most-used
+ * columns (as many as fit in shared memory beside the staging buffers, and
+ * only if they take >= 25% of the nonzeros) are staged in shared memory at
+ * kernel start, and the plan keeps a copy of colidx with those columns
+ * remapped — so such a plan snapshots the column indices of A, and must be
+ * rebuilt if they change. block 128/256/512 select the tile-per-warp grid
+ * kernel with a separate fix-up kernel. Results are bit-identical across
+ * all forms. SpMVs that share one plan must not overlap on the GPU (the
+ * plan owns the carry scratch). */
 int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stream, mr_merbit_plan** plan);
+#define MR_PLAN_NO_HUB_CACHE 1    /* never build the shared-memory hub cache */
+#define MR_PLAN_GATHER_NO_L1 2    /* x gathers do not allocate L1 lines */
+#define MR_PLAN_GATHER_L2_ONLY 4  /* x gathers read through L2 only (.cg) */
+#define MR_PLAN_SMALL_HUB_CACHE 8 /* at most 8192 hub columns (leaves L1 room) */
+#define MR_PLAN_HUB_LIMIT(kcols) ((int)(kcols) << 8) /* at most kcols * 1024 hub columns */
+/* As mr_merbit_plan_create, with tuning flags (MR_PLAN_*); every flag
+ * combination computes the same bits. */
+int mr_merbit_plan_create_ex(const mr_csr_view* A, int sigma, int block, int flags, void* stream,
+                             mr_merbit_plan** plan);
 /* Replaces TILE::~TILE (include/merbit.cuh:256-263). Synchronises the device
  * before freeing. */
 int mr_merbit_plan_destroy(mr_merbit_plan* plan);
@@ -160,19 +183,67 @@ int mr_batch_info(const mr_batch* batch, int32_t* groups, int64_t* total_tiles);
 int mr_batch_destroy(mr_batch* batch);
 
 /* Autotuner over MERBIT's tile size (sigma: items per lane, the tile is
- * 32 x sigma merge items) and threads per CTA (block): times every supported
- * pair on A (median of reps) and returns the fastest. The reference
+ * 32 x sigma merge items), threads per CTA (block) and the hub cache: times
+ * every supported combination on A (median of reps) and returns the fastest
+ * as (sigma, block, plan flags for mr_merbit_plan_create_ex). The reference
  * hard-codes BLOCK 256, SIGMA 14 (src/class.cu:1409-1410). */
 int mr_autotune_merbit(const mr_csr_view* A, const float* x_dev, float* y_dev, int32_t reps, int32_t* best_sigma,
-                       int32_t* best_block, float* best_ms, void* stream);
+                       int32_t* best_block, int32_t* best_flags, float* best_ms, void* stream);
 /* Size-bucketed cache of tuning results: bucket = (floor(log2 rows),
  * floor(log2 mean row length)); a miss tunes on the given matrix. */
 typedef struct mr_tuner mr_tuner;
 int mr_tuner_create(mr_tuner** tuner);
 int mr_tuner_destroy(mr_tuner* tuner);
 int mr_tuner_pick(mr_tuner* tuner, const mr_csr_view* A, const float* x_dev, float* y_dev, int32_t* sigma,
-                  int32_t* block, void* stream);
+                  int32_t* block, int32_t* flags, void* stream);
 int mr_tuner_stats(mr_tuner* tuner, int32_t* buckets, int32_t* tuned);
+
+/* ------------------------------------------------------- serving ---- */
+
+/* Continuous-batching SpMV server over a device-resident pool of matrices.
+ * No reference counterpart (the reference runs one matrix per process);
+ * this is the serving form of the path. Matrices are registered with host
+ * CSR arrays that the caller keeps alive, optionally with the permutation
+ * perm[old] = new the matrix was reordered with; requests then carry x in
+ * the original numbering and receive y in it. A matrix is uploaded and
+ * planned on first use, within hbm_budget_bytes, evicting the least
+ * recently used idle matrices. A scheduler thread batches the requests that
+ * arrive within window_us of the first pending one (at most max_batch) and
+ * keeps up to `lanes` batches in flight on separate streams. Each request's
+ * result is bitwise the same alone or in any batch. */
+typedef struct mr_server mr_server;
+typedef struct mr_server_config {
+    int64_t hbm_budget_bytes; /* device bytes for resident matrices; 0 = half the free memory */
+    int32_t window_us;        /* batching window (default 200) */
+    int32_t max_batch;        /* requests per batch (default 256) */
+    int32_t lanes;            /* batches in flight, one stream each (default 3) */
+    int32_t sigma;            /* MERBIT sigma of resident plans (default 14) */
+} mr_server_config;
+typedef struct mr_server_stats {
+    int64_t submitted, completed, rejected, batches, admissions, evictions;
+    int64_t resident_bytes, resident_matrices;
+    double mean_batch;
+    double p50_us, p99_us, mean_us, max_us; /* latency: submit -> result in y */
+    double req_per_s;                       /* completed / (last completion - first submit) */
+} mr_server_stats;
+
+int mr_server_create(const mr_server_config* cfg, mr_server** server);
+int mr_server_add_matrix(mr_server* server, int32_t n, int64_t nnz, const int32_t* rowptr_host,
+                         const int32_t* colidx_host, const void* vals_host, int32_t dtype,
+                         const int32_t* perm_old2new_host, int32_t* id);
+/* Queues y = A_id x; x_host must stay valid and y_host writable until the
+ * request completes (mr_server_wait / mr_server_drain). */
+int mr_server_submit(mr_server* server, int32_t id, const float* x_host, float* y_host, uint64_t* ticket);
+/* Waits up to timeout_ms (MR_ERR_TIMEOUT after); returns the request's status. */
+int mr_server_wait(mr_server* server, uint64_t ticket, int32_t timeout_ms, double* latency_us);
+int mr_server_drain(mr_server* server, int32_t timeout_ms);
+int mr_server_get_stats(mr_server* server, mr_server_stats* stats);
+int mr_server_reset_stats(mr_server* server);
+int mr_server_destroy(mr_server* server);
+/* Open-loop Poisson load generator: n_requests arrivals at `rate` per second
+ * over the ids (uniform), x_of[k] / y_of[k] host buffers of ids[k]. */
+int mr_server_loadgen(mr_server* server, const int32_t* ids, int32_t n_ids, int64_t n_requests, double rate,
+                      uint64_t seed, const float* const* x_of, float* const* y_of, int32_t timeout_ms);
 
 /* ------------------------------------------------------ permutation ---- */
 

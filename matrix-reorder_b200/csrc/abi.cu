@@ -70,6 +70,12 @@ int mr_spmv_csr(const mr_csr_view* A, const float* x, float* y, void* stream)
 
 int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stream, mr_merbit_plan** out)
 {
+    return mr_merbit_plan_create_ex(A, sigma, block, 0, stream, out);
+}
+
+int mr_merbit_plan_create_ex(const mr_csr_view* A, int sigma, int block, int flags, void* stream,
+                             mr_merbit_plan** out)
+{
     if (!out) return MR_ERR_INVALID_ARG;
     *out = nullptr;
     MR_TRY(check_view(A, false));
@@ -102,6 +108,8 @@ int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stre
         cudaFree(p.lane_desc);
         cudaFree(p.carry);
         cudaFree(p.ticket);
+        cudaFree(p.colh);
+        cudaFree(p.hub_cols);
         delete h;
         return code;
     };
@@ -117,6 +125,13 @@ int mr_merbit_plan_create(const mr_csr_view* A, int sigma, int block, void* stre
     int s = launch_merbit_plan(A->rowptr, A->n_rows, (int)A->nnz, sigma, p.lane_num, p.tile_num, p.tile_x, p.tile_y,
                                p.lane_desc, st);
     if (s != MR_OK) return fail(s);
+    p.gather_mode = (flags & MR_PLAN_GATHER_NO_L1) ? 1 : (flags & MR_PLAN_GATHER_L2_ONLY) ? 2 : 0;
+    if (flags & MR_PLAN_SMALL_HUB_CACHE) p.hub_limit = 8192;
+    if ((flags >> 8) & 0xffff) p.hub_limit = 1024 * ((flags >> 8) & 0xffff);
+    if (block == 1024 && !(flags & MR_PLAN_NO_HUB_CACHE)) {
+        s = build_hub_cache(p, *A, st);
+        if (s != MR_OK) return fail(s);
+    }
     *out = h;
     return MR_OK;
 }
@@ -133,6 +148,8 @@ int mr_merbit_plan_destroy(mr_merbit_plan* h)
     cudaFree(h->p.lane_desc);
     cudaFree(h->p.carry);
     cudaFree(h->p.ticket);
+    cudaFree(h->p.colh);
+    cudaFree(h->p.hub_cols);
     if (dev != h->p.device) cudaSetDevice(dev);
     delete h;
     return MR_OK;
@@ -152,6 +169,8 @@ int mr_merbit_plan_get_info(const mr_merbit_plan* h, mr_merbit_plan_info* info)
     info->tile_x_dev = p.tile_x;
     info->tile_y_dev = p.tile_y;
     info->lane_desc_dev = p.lane_desc;
+    info->hub_columns = p.hub_k;
+    info->hub_coverage = p.hub_coverage;
     return MR_OK;
 }
 

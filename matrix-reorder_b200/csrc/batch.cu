@@ -13,6 +13,7 @@
 // Changing an item's x/y pointers rewrites the device table only, so a
 // captured graph stays valid.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstring>
 #include <cmath>
@@ -115,6 +116,8 @@ void fill_op(unsigned char* dst, const MerbitPlan& p, const mr_csr_view& A, cons
     op.m.x = x;
     op.m.y = y;
     op.m.carry = carry;
+    op.m.hub = nullptr;
+    op.m.gather_mode = p.gather_mode;
     op.m.vec_ok = ((reinterpret_cast<uintptr_t>(A.colidx) & 15) == 0) &&
                   ((reinterpret_cast<uintptr_t>(A.vals) & (4 * sizeof(V) - 1)) == 0);
     op.tile_num = p.tile_num;
@@ -180,6 +183,38 @@ struct FillF {
 };
 
 }  // namespace
+
+namespace mr {
+
+// internal entry points for other host components (the serving loop)
+size_t batch_op_bytes(int dtype, int sigma) { return (size_t)dispatch(dtype, sigma, OpSizeF{}); }
+
+int batch_fill_op(void* dst, int dtype, int sigma, const MerbitPlan& p, const mr_csr_view& A, const float* x, float* y,
+                  float* carry)
+{
+    FillF f{static_cast<unsigned char*>(dst), &p, &A, x, y, carry};
+    return dispatch(dtype, sigma, f);
+}
+
+int batch_launch_ops(int dtype, int sigma, const void* d_ops, const long long* d_prefix, int count,
+                     long long total_tiles, cudaStream_t st)
+{
+    Group g;
+    g.dtype = dtype;
+    g.sigma = sigma;
+    g.items.resize((size_t)count);
+    g.ops = const_cast<void*>(d_ops);
+    g.prefix = const_cast<long long*>(d_prefix);
+    g.total_tiles = total_tiles;
+    g.grid = (int)std::max<long long>(
+        1, std::min<long long>((total_tiles + kBatchWarps - 1) / kBatchWarps, (long long)sm_count() * 4));
+    const int rc = dispatch(dtype, sigma, LaunchF{&g, st});
+    g.ops = nullptr;
+    g.prefix = nullptr;
+    return rc;
+}
+
+}  // namespace mr
 
 struct mr_batch {
     std::vector<mr_batch_item> items;
@@ -377,43 +412,65 @@ int mr_batch_destroy(mr_batch* b)
 // ------------------------------------------------------------- autotuner ---
 
 int mr_autotune_merbit(const mr_csr_view* A, const float* x, float* y, int32_t reps, int32_t* best_sigma,
-                       int32_t* best_block, float* best_ms, void* stream)
+                       int32_t* best_block, int32_t* best_flags, float* best_ms, void* stream)
 {
     if (!A || !best_sigma || !best_block) return MR_ERR_INVALID_ARG;
     static const int sigmas[] = {7, 10, 14, 16, 20, 24, 28, 32};
-    static const int blocks[] = {128, 256, 512, 1024};
     if (reps < 1) reps = 5;
     cudaStream_t st = as_stream(stream);
     cudaEvent_t e0, e1;
     MR_CUDA_TRY(cudaEventCreate(&e0));
     MR_CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
-    int bs = 14, bb = 256;
+    int bs = 14, bb = 1024, bf = 0;
     int status = MR_OK;
-    for (int s : sigmas) {
-        mr_merbit_plan* plan = nullptr;
-        status = mr_merbit_plan_create(A, s, 1024, stream, &plan);
-        if (status != MR_OK) break;
-        for (int blk : blocks) {
-            plan->p.block = blk;
-            status = mr_spmv_merbit(plan, A, x, y, stream);  // warm
-            std::vector<float> t;
-            for (int r = 0; r < reps && status == MR_OK; ++r) {
-                cudaEventRecord(e0, st);
-                status = mr_spmv_merbit(plan, A, x, y, stream);
-                cudaEventRecord(e1, st);
-                cudaEventSynchronize(e1);
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                t.push_back(ms);
-            }
-            if (status != MR_OK) break;
+    auto time_plan = [&](mr_merbit_plan* plan, float* out) {
+        int rc = mr_spmv_merbit(plan, A, x, y, stream);  // warm
+        std::vector<float> t;
+        for (int r = 0; r < reps && rc == MR_OK; ++r) {
+            cudaEventRecord(e0, st);
+            rc = mr_spmv_merbit(plan, A, x, y, stream);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t.push_back(ms);
+        }
+        if (rc == MR_OK) {
             std::nth_element(t.begin(), t.begin() + t.size() / 2, t.end());
-            const float med = t[t.size() / 2];
-            if (med < best) {
-                best = med;
+            *out = t[t.size() / 2];
+        }
+        return rc;
+    };
+    for (int s : sigmas) {
+        // (a) persistent kernel with its hub cache (when the plan builds one)
+        mr_merbit_plan* plan = nullptr;
+        status = mr_merbit_plan_create_ex(A, s, 1024, 0, stream, &plan);
+        if (status != MR_OK) break;
+        const bool has_hub = plan->p.hub_k > 0;
+        float ms = 0.f;
+        status = time_plan(plan, &ms);
+        mr_merbit_plan_destroy(plan);
+        if (status != MR_OK) break;
+        if (ms < best) {
+            best = ms;
+            bs = s;
+            bb = 1024;
+            bf = 0;
+        }
+        // (b) without a hub cache, every CTA shape
+        status = mr_merbit_plan_create_ex(A, s, 1024, MR_PLAN_NO_HUB_CACHE, stream, &plan);
+        if (status != MR_OK) break;
+        for (int blk : {128, 256, 512, 1024}) {
+            if (blk == 1024 && !has_hub) continue;  // same kernel as (a)
+            plan->p.block = blk;
+            status = time_plan(plan, &ms);
+            if (status != MR_OK) break;
+            if (ms < best) {
+                best = ms;
                 bs = s;
                 bb = blk;
+                bf = MR_PLAN_NO_HUB_CACHE;
             }
         }
         mr_merbit_plan_destroy(plan);
@@ -424,6 +481,7 @@ int mr_autotune_merbit(const mr_csr_view* A, const float* x, float* y, int32_t r
     if (status != MR_OK) return status;
     *best_sigma = bs;
     *best_block = bb;
+    if (best_flags) *best_flags = bf;
     if (best_ms) *best_ms = best;
     return MR_OK;
 }
@@ -434,7 +492,7 @@ int mr_autotune_merbit(const mr_csr_view* A, const float* x, float* y, int32_t r
 // length)); the first matrix of a bucket is tuned, later ones reuse it.
 struct mr_tuner {
     std::mutex mu;
-    std::map<std::pair<int, int>, std::pair<int, int>> best;
+    std::map<std::pair<int, int>, std::array<int, 3>> best;  // sigma, block, flags
     int tuned = 0;
 };
 
@@ -462,7 +520,7 @@ int mr_tuner_destroy(mr_tuner* t)
 }
 
 int mr_tuner_pick(mr_tuner* t, const mr_csr_view* A, const float* x, float* y, int32_t* sigma, int32_t* block,
-                  void* stream)
+                  int32_t* flags, void* stream)
 {
     if (!t || !A || !sigma || !block) return MR_ERR_INVALID_ARG;
     const auto key = bucket_of(A);
@@ -470,18 +528,20 @@ int mr_tuner_pick(mr_tuner* t, const mr_csr_view* A, const float* x, float* y, i
         std::lock_guard<std::mutex> lk(t->mu);
         auto f = t->best.find(key);
         if (f != t->best.end()) {
-            *sigma = f->second.first;
-            *block = f->second.second;
+            *sigma = f->second[0];
+            *block = f->second[1];
+            if (flags) *flags = f->second[2];
             return MR_OK;
         }
     }
-    int s = 14, b = 1024;
-    MR_TRY(mr_autotune_merbit(A, x, y, 5, &s, &b, nullptr, stream));
+    int s = 14, b = 1024, fl = 0;
+    MR_TRY(mr_autotune_merbit(A, x, y, 5, &s, &b, &fl, nullptr, stream));
     std::lock_guard<std::mutex> lk(t->mu);
-    t->best[key] = {s, b};
+    t->best[key] = {s, b, fl};
     ++t->tuned;
     *sigma = s;
     *block = b;
+    if (flags) *flags = fl;
     return MR_OK;
 }
 

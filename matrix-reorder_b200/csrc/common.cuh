@@ -174,6 +174,20 @@ __device__ __forceinline__ float ld_x(const float* p, uint64_t pol)
 __host__ __device__ __forceinline__ int64_t min64(int64_t a, int64_t b) { return a < b ? a : b; }
 __host__ __device__ __forceinline__ int64_t max64(int64_t a, int64_t b) { return a > b ? a : b; }
 
+// x gather variants: 0 = read-only path, allocate in L1; 1 = read-only
+// path without L1 allocation; 2 = L2 only (.cg). All keep the line in L2.
+__device__ __forceinline__ float ld_x_mode(const float* p, uint64_t pol, int mode)
+{
+    float v;
+    if (mode == 1)
+        asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    else if (mode == 2)
+        asm("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    else
+        asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 // ---- warp helpers ----------------------------------------------------------
 __device__ __forceinline__ float warp_sum(float v)
 {

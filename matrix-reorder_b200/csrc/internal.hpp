@@ -23,6 +23,15 @@ struct MerbitPlan {
     void* lane_desc = nullptr;    // lane_num words (4 or 8 bytes)
     float* carry = nullptr;       // tile_num carries
     int* ticket = nullptr;        // persistent kernel's completion counter (starts at 0)
+    // hub cache (persistent kernel only): the most-used columns' x values are
+    // staged in shared memory; colh is the plan's copy of colidx with hub
+    // columns replaced by (0x80000000 | slot); hub_cols[slot] = column
+    int32_t* colh = nullptr;
+    int32_t* hub_cols = nullptr;
+    int hub_k = 0;
+    double hub_coverage = 0.0;    // share of nonzeros whose column is a hub
+    int hub_limit = 0;            // cap on hub slots (0: as many as fit)
+    int gather_mode = 0;          // x gather cache path (ld_x_mode)
     int device = 0;
 };
 
@@ -31,9 +40,20 @@ int launch_merbit_plan(const int* rowptr, int nrow, int nnz, int sigma, int lane
 int launch_merbit_spmv(const MerbitPlan& p, const int* colidx, const void* vals, int dtype, const float* x, float* y,
                        float* carry, cudaStream_t st);
 bool merbit_sigma_supported(int sigma);
+// builds the hub cache of a persistent-kernel plan (no-op when it would not pay)
+int build_hub_cache(MerbitPlan& p, const mr_csr_view& A, cudaStream_t st);
+// largest number of hub slots that fit beside the SIGMA staging buffers
+int hub_capacity(int sigma);
 
 int launch_csr_spmv(int n, int64_t nnz, const int* rowptr, const int* colidx, const void* vals, int dtype,
                     const float* x, float* y, cudaStream_t st);
+
+// batched SpMV internals (operand tables built by the caller)
+size_t batch_op_bytes(int dtype, int sigma);
+int batch_fill_op(void* dst, int dtype, int sigma, const MerbitPlan& p, const mr_csr_view& A, const float* x, float* y,
+                  float* carry);
+int batch_launch_ops(int dtype, int sigma, const void* d_ops, const long long* d_prefix, int count,
+                     long long total_tiles, cudaStream_t st);
 
 // permutation
 int permute_csr(const mr_csr_view& A, const int32_t* perm, int32_t* out_rowptr, int32_t* out_colidx, void* out_vals,

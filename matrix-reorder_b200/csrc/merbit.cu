@@ -23,6 +23,7 @@
 //    FP64 in tile order. Results are bitwise reproducible run to run.
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -204,9 +205,10 @@ __device__ __forceinline__ void fixup_boundary(const uint32_t* __restrict__ tile
     y[R] = (float)((double)__ldcg(y + R) + acc);
 }
 
-template <typename V, int SIGMA>
+template <typename V, int SIGMA, bool HUB>
 __global__ void __launch_bounds__(kPersistWarps * 32, 1)
-    merbit_persistent_kernel(const MerbitOperand<V, SIGMA> m, int tile_num, int nrow, int* __restrict__ ticket)
+    merbit_persistent_kernel(const MerbitOperand<V, SIGMA> m_in, int tile_num, int nrow, int* __restrict__ ticket,
+                             const int32_t* __restrict__ hub_cols, int hub_k)
 {
     extern __shared__ __align__(16) float s_dyn[];
     __shared__ int s_last;
@@ -217,7 +219,32 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     const int t1 = min(t0 + chunk, tile_num);
     float* s = s_dyn + warp * tile_smem_words<SIGMA>();
     const TilePolicy pol{l2_evict_last_policy(), l2_evict_first_policy()};
-    for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true>(m, t, s, pol);
+    MerbitOperand<V, SIGMA> m = m_in;
+    if constexpr (HUB) {
+        // stage x of the hub columns once per CTA
+        float* hub = s_dyn + kPersistWarps * tile_smem_words<SIGMA>();
+        // 16 independent gathers in flight per thread
+        constexpr int PF = 16;
+        for (int base = threadIdx.x; base < hub_k; base += blockDim.x * PF) {
+            int c[PF];
+            float v[PF];
+#pragma unroll
+            for (int j = 0; j < PF; ++j) {
+                const int i = base + j * (int)blockDim.x;
+                c[j] = i < hub_k ? __ldg(hub_cols + i) : -1;
+            }
+#pragma unroll
+            for (int j = 0; j < PF; ++j) v[j] = c[j] >= 0 ? ld_x(m.x + c[j], pol.x_keep) : 0.f;
+#pragma unroll
+            for (int j = 0; j < PF; ++j) {
+                const int i = base + j * (int)blockDim.x;
+                if (i < hub_k) hub[i] = v[j];
+            }
+        }
+        m.hub = hub;
+        __syncthreads();
+    }
+    for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true, HUB>(m, t, s, pol);
     __syncthreads();
     for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x) fixup_in_chunk(m.tile_y, m.carry, t0, t1, nrow, m.y, t);
     __threadfence();
@@ -257,6 +284,8 @@ static int launch_spmv_t(const MerbitPlan& p, const int* colidx, const void* val
     m.y = y;
     m.carry = carry;
     m.vec_ok = vec_ok;
+    m.hub = nullptr;
+    m.gather_mode = p.gather_mode;
     if (grid > 0) merbit_spmv_kernel<V, SIGMA, WARPS><<<grid, WARPS * 32, 0, st>>>(m, p.tile_num);
     MR_CUDA_TRY(cudaGetLastError());
     if (p.tile_num > 0) {
@@ -278,30 +307,195 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
     m.lane_num = p.lane_num;
     m.nnz = nnz;
     m.items = (int64_t)p.n_rows + p.nnz;
-    m.colidx = colidx;
+    const int* cols = p.hub_k > 0 ? p.colh : colidx;  // hub plans read their remapped copy
+    m.colidx = cols;
     m.vals = reinterpret_cast<const V*>(vals);
     m.x = x;
     m.y = y;
     m.carry = carry;
-    m.vec_ok = ((reinterpret_cast<uintptr_t>(colidx) & 15) == 0) &&
+    m.vec_ok = ((reinterpret_cast<uintptr_t>(cols) & 15) == 0) &&
                ((reinterpret_cast<uintptr_t>(vals) & (4 * sizeof(V) - 1)) == 0);
-    const size_t smem = sizeof(float) * (size_t)kPersistWarps * tile_smem_words<SIGMA>();
-    static bool configured = false;  // per instantiation; attributes are per device but idempotent
-    if (!configured) {
-        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        // smallest shared-memory carve-out that fits: the rest of the SM's
-        // 256 KB stays L1 for x
-        const int pct = (int)((smem + 1023) / 1024 * 100 / 228) + 1;
-        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA>,
-                                         cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100)));
-        configured = true;
-    }
+    m.hub = nullptr;
+    m.gather_mode = p.gather_mode;
+    const size_t stage = sizeof(float) * (size_t)kPersistWarps * tile_smem_words<SIGMA>();
     const int grid = std::max(1, std::min(sm_count(), (p.tile_num + kPersistWarps - 1) / kPersistWarps));
-    merbit_persistent_kernel<V, SIGMA><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows, p.ticket);
+    if (p.hub_k > 0) {
+        const size_t smem = stage + sizeof(float) * (size_t)p.hub_k;
+        static std::once_flag once;
+        static cudaError_t cfg = cudaSuccess;
+        std::call_once(once, [&] {
+            int optin = 0, dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            cudaFuncAttributes fa;
+            cfg = cudaFuncGetAttributes(&fa, merbit_persistent_kernel<V, SIGMA, true>);
+            // static and dynamic shared memory together may not exceed the opt-in limit
+            if (cfg == cudaSuccess)
+                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           optin - (int)fa.sharedSizeBytes);
+        });
+        MR_CUDA_TRY(cfg);
+        // carve-out sized to this plan's shared memory: the rest stays L1
+        const int pct = std::min(100, (int)((smem + 1023) / 1024 * 100 / 228) + 1);
+        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true>,
+                                         cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+        merbit_persistent_kernel<V, SIGMA, true><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows,
+                                                                                        p.ticket, p.hub_cols, p.hub_k);
+    } else {
+        static std::once_flag once;
+        static cudaError_t cfg = cudaSuccess;
+        std::call_once(once, [&] {
+            cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+            // smallest shared-memory carve-out that fits: the rest of the
+            // SM's 256 KB stays L1 for x
+            const int pct = (int)((stage + 1023) / 1024 * 100 / 228) + 1;
+            if (cfg == cudaSuccess)
+                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100));
+        });
+        MR_CUDA_TRY(cfg);
+        merbit_persistent_kernel<V, SIGMA, false><<<grid, kPersistWarps * 32, stage, st>>>(m, p.tile_num, p.n_rows,
+                                                                                          p.ticket, nullptr, 0);
+    }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
 }
+
+// ------------------------------------------------------------ hub cache ----
+
+__global__ void col_count_kernel(const int32_t* __restrict__ colidx, int64_t nnz, int32_t* __restrict__ cnt)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[colidx[k]], 1);
+}
+
+constexpr int kCountCap = 1 << 16;
+
+// histogram of column counts (counts >= kCountCap share the last bucket)
+__global__ void count_hist_kernel(const int32_t* __restrict__ cnt, int ncols, unsigned long long* __restrict__ h,
+                                  unsigned long long* __restrict__ hw)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x) {
+        const int v = cnt[c];
+        if (v >= 2) {
+            atomicAdd(&h[min(v, kCountCap)], 1ull);
+            atomicAdd(&hw[min(v, kCountCap)], (unsigned long long)v);
+        }
+    }
+}
+
+__global__ void hub_flag_kernel(const int32_t* __restrict__ cnt, int ncols, int thr, int32_t* __restrict__ flag)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x)
+        flag[c] = cnt[c] >= thr ? 1 : 0;
+}
+
+// slot = exclusive scan of the flags; hub_cols[slot] = c; slot_of[c] = slot or -1
+__global__ void hub_slots_kernel(const int32_t* __restrict__ flag, const int32_t* __restrict__ scan, int ncols,
+                                 int32_t* __restrict__ hub_cols, int32_t* __restrict__ slot_of)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncols; c += gridDim.x * blockDim.x) {
+        if (flag[c]) {
+            hub_cols[scan[c]] = c;
+            slot_of[c] = scan[c];
+        } else {
+            slot_of[c] = -1;
+        }
+    }
+}
+
+__global__ void hub_remap_kernel(const int32_t* __restrict__ colidx, int64_t nnz, const int32_t* __restrict__ slot_of,
+                                 int32_t* __restrict__ colh)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+        const int c = colidx[k];
+        const int s = slot_of[c];
+        colh[k] = s >= 0 ? (int)(0x80000000u | (uint32_t)s) : c;
+    }
+}
+
+}  // namespace mr
+
+namespace mr {
+
+int hub_capacity(int sigma)
+{
+    int optin = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const long long stage = 4ll * kPersistWarps * (32 * sigma + 8);
+    // leave 64 KB of the SM's memory as L1: the x gathers that miss the hub
+    // cache need it (measured on R-MAT s22: below ~40 KB of L1 the kernel
+    // slows down by a third whatever the hub coverage)
+    const long long room = (long long)optin - stage - 65536 - 1024;
+    if (room <= 0) return 0;
+    return (int)std::min<long long>(room / 4 / 128 * 128, 1 << 20);
+}
+
+int build_hub_cache(MerbitPlan& p, const mr_csr_view& A, cudaStream_t st)
+{
+    p.hub_k = 0;
+    p.hub_coverage = 0.0;
+    int cap = hub_capacity(p.sigma);
+    if (p.hub_limit > 0) cap = std::min(cap, p.hub_limit);
+    if (cap < 1024 || A.nnz < (1 << 16) || A.n_cols <= 0) return MR_OK;
+    const int ncols = A.n_cols;
+    const int grid_c = (int)std::min<int64_t>(((int64_t)ncols + 255) / 256, (int64_t)sm_count() * 8);
+    const int grid_k = (int)std::min<int64_t>((A.nnz + 255) / 256, (int64_t)sm_count() * 16);
+    DevBuf cnt, hist, flag, scan, slot_of;
+    MR_TRY(cnt.alloc(sizeof(int32_t) * (size_t)ncols, st));
+    MR_TRY(hist.alloc(sizeof(unsigned long long) * 2 * (kCountCap + 1), st));
+    MR_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, sizeof(int32_t) * (size_t)ncols, st));
+    MR_CUDA_TRY(cudaMemsetAsync(hist.p, 0, sizeof(unsigned long long) * 2 * (kCountCap + 1), st));
+    col_count_kernel<<<grid_k, 256, 0, st>>>(A.colidx, A.nnz, cnt.as<int32_t>());
+    unsigned long long* h = hist.as<unsigned long long>();
+    count_hist_kernel<<<grid_c, 256, 0, st>>>(cnt.as<int32_t>(), ncols, h, h + kCountCap + 1);
+    MR_CUDA_TRY(cudaGetLastError());
+    std::vector<unsigned long long> hh(2 * (kCountCap + 1));
+    MR_CUDA_TRY(cudaMemcpyAsync(hh.data(), h, sizeof(unsigned long long) * hh.size(), cudaMemcpyDeviceToHost, st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));
+    // smallest threshold thr >= 2 whose column set {count >= thr} fits
+    unsigned long long ncol = 0, weight = 0;
+    int thr = kCountCap + 1;
+    for (int c = kCountCap; c >= 2; --c) {
+        if (ncol + hh[(size_t)c] > (unsigned long long)cap) break;
+        ncol += hh[(size_t)c];
+        weight += hh[(size_t)(kCountCap + 1 + c)];
+        thr = c;
+    }
+    const double coverage = (double)weight / (double)A.nnz;
+    // a hub cache that serves few gathers is not worth its shared memory
+    // (the L1 it displaces would serve them as well): below 20% of the
+    // nonzeros the plan runs without it
+    if (ncol == 0 || coverage < 0.20) return MR_OK;
+    MR_TRY(flag.alloc(sizeof(int32_t) * (size_t)ncols, st));
+    MR_TRY(scan.alloc(sizeof(int32_t) * ((size_t)ncols + 1), st));
+    MR_TRY(slot_of.alloc(sizeof(int32_t) * (size_t)ncols, st));
+    hub_flag_kernel<<<grid_c, 256, 0, st>>>(cnt.as<int32_t>(), ncols, thr, flag.as<int32_t>());
+    MR_TRY(exclusive_scan_i32(flag.as<int32_t>(), scan.as<int32_t>(), ncols, st));
+    if (cudaMalloc(&p.hub_cols, sizeof(int32_t) * (size_t)ncol) != cudaSuccess ||
+        cudaMalloc(&p.colh, sizeof(int32_t) * (size_t)A.nnz) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p.hub_cols);
+        cudaFree(p.colh);
+        p.hub_cols = nullptr;
+        p.colh = nullptr;
+        return MR_OK;  // no room for the cache: run without it
+    }
+    hub_slots_kernel<<<grid_c, 256, 0, st>>>(flag.as<int32_t>(), scan.as<int32_t>(), ncols, p.hub_cols,
+                                            slot_of.as<int32_t>());
+    hub_remap_kernel<<<grid_k, 256, 0, st>>>(A.colidx, A.nnz, slot_of.as<int32_t>(), p.colh);
+    MR_CUDA_TRY(cudaGetLastError());
+    p.hub_k = (int)ncol;
+    p.hub_coverage = coverage;
+    return MR_OK;
+}
+
+}  // namespace mr
+
+namespace mr {
 
 template <typename V, int SIGMA>
 static int launch_spmv_w(const MerbitPlan& p, const int* colidx, const void* vals, int nnz, const float* x, float* y,

@@ -48,6 +48,8 @@ template <typename V, int SIGMA> struct MerbitOperand {
     float* y;
     float* carry;
     int vec_ok;     // colidx/vals aligned for vector loads
+    const float* hub;  // shared-memory x values of hub columns, or nullptr
+    int gather_mode;   // ld_x_mode variant of the x gathers
 };
 
 // Cache policies of one tile: x gathers keep their lines in L2 (evict-last);
@@ -66,7 +68,7 @@ template <bool NA, typename T> __device__ __forceinline__ T ld_s(const T* p, uin
         return ld_stream(p);
 }
 
-template <typename V, int SIGMA, bool NA = false>
+template <typename V, int SIGMA, bool NA = false, bool HUB = false>
 __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, const int tile, float* __restrict__ s,
                                             const TilePolicy pols)
 {
@@ -135,8 +137,16 @@ __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, co
                 const int k = a0 + 4 * v;
                 float p[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    p[j] = (k + j >= x0 && k + j < x1) ? val[u][j] * ld_x(m.x + col[u][j], pol) : 0.f;
+                for (int j = 0; j < 4; ++j) {
+                    p[j] = 0.f;
+                    if (k + j >= x0 && k + j < x1) {
+                        const int c = col[u][j];
+                        if constexpr (HUB)  // hub columns carry the sign bit and read shared memory
+                            p[j] = val[u][j] * ((c < 0) ? m.hub[c & 0x7fffffff] : ld_x_mode(m.x + c, pol, m.gather_mode));
+                        else
+                            p[j] = val[u][j] * ld_x_mode(m.x + c, pol, m.gather_mode);
+                    }
+                }
                 if (single_row)
                     part += (p[0] + p[1]) + (p[2] + p[3]);
                 else

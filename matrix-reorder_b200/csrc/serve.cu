@@ -1,0 +1,751 @@
+// Serving loop: device-resident pool of (reordered) matrices, continuous
+// batching of SpMV requests, p50/p99 latency.
+//
+// No counterpart in the reference (a one-matrix-per-process harness); this is
+// the serving form BASELINE.json's north_star asks for.
+//
+//  * Pool: matrices are registered with host CSR arrays (borrowed: the caller
+//    keeps them alive) and an optional permutation perm[old] = new; requests
+//    then use the original numbering and the server applies x' = P x and
+//    y = P^T y'. A matrix becomes resident on first use: upload + MERBIT plan
+//    into stream-ordered device memory, admitted against an HBM budget, the
+//    least recently used idle matrices evicted first.
+//  * Batching: a scheduler thread waits `window_us` after the first pending
+//    request (or until max_batch are pending), takes the pending requests in
+//    arrival order, admits their matrices and launches the batch on a free
+//    lane (stream); up to `lanes` batches are in flight, so requests that
+//    arrive while others are on the GPU form the next batch and overlap on
+//    the device (continuous batching). A batch is: one H2D copy of all x,
+//    one batched permutation, the batched MERBIT kernels (one per (sigma,
+//    dtype) group), one batched un-permutation, one D2H copy.
+//  * Completion: a thread waits on each lane's event in launch order, copies
+//    results to the callers' y, records latency (submit -> result in y).
+//  * Determinism: every request's SpMV runs the same tiles with the same
+//    order of operations whatever else is in its batch, so its result is
+//    bitwise the same alone and in the mix.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <random>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+using namespace mr;
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct PermOp {
+    const int32_t* perm;  // nullptr: identity
+    long long off;        // offset of this item's vector in the batch arena
+    int n;
+};
+
+// item owning position g: largest i with prefix[i] <= g
+__device__ __forceinline__ int find_seg(const long long* __restrict__ prefix, int count, long long g)
+{
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// inverse == 0: out[off + perm[i]] = in[off + i]; else out[off + i] = in[off + perm[i]]
+__global__ void batch_permute_kernel(const PermOp* __restrict__ ops, const long long* __restrict__ prefix, int count,
+                                     long long total, const float* __restrict__ in, float* __restrict__ out,
+                                     int inverse)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const PermOp op = ops[find_seg(prefix, count, g)];
+        const int i = (int)(g - op.off);
+        if (!op.perm) {
+            out[g] = in[g];
+        } else {
+            const int p = op.perm[i];
+            if (inverse)
+                out[g] = in[op.off + p];
+            else
+                out[op.off + p] = in[g];
+        }
+    }
+}
+
+struct Request {
+    uint64_t ticket = 0;
+    int id = 0;
+    const float* x = nullptr;
+    float* y = nullptr;
+    Clock::time_point t_submit;
+    double latency_us = 0.0;
+    int status = MR_OK;
+    bool done = false;
+};
+
+struct Matrix {
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int dtype = MR_F32;
+    const int32_t* h_rowptr = nullptr;
+    const int32_t* h_colidx = nullptr;
+    const void* h_vals = nullptr;
+    const int32_t* h_perm = nullptr;
+    // device state while resident
+    bool resident = false;
+    int refs = 0;
+    uint64_t last_use = 0;
+    size_t bytes = 0;
+    int32_t* d_rowptr = nullptr;
+    int32_t* d_colidx = nullptr;
+    void* d_vals = nullptr;
+    int32_t* d_perm = nullptr;
+    MerbitPlan plan;
+};
+
+template <typename T> struct PinnedVec {
+    T* p = nullptr;
+    size_t cap = 0;
+    int reserve(size_t n)
+    {
+        if (n <= cap) return MR_OK;
+        size_t c = std::max(n, cap * 2);
+        T* q = nullptr;
+        if (cudaHostAlloc(&q, sizeof(T) * c, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return MR_ERR_NOMEM;
+        }
+        if (p) cudaFreeHost(p);
+        p = q;
+        cap = c;
+        return MR_OK;
+    }
+    ~PinnedVec()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+struct DevVec {
+    void* p = nullptr;
+    size_t cap = 0;  // bytes
+    int reserve(size_t bytes, cudaStream_t st)
+    {
+        if (bytes <= cap) return MR_OK;
+        size_t c = std::max(bytes, cap * 2);
+        if (p) cudaFreeAsync(p, st);
+        p = nullptr;
+        cap = 0;
+        if (cudaMallocAsync(&p, c, st) != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            return MR_ERR_NOMEM;
+        }
+        cap = c;
+        return MR_OK;
+    }
+};
+
+struct Lane {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    PinnedVec<float> hx, hy;
+    DevVec dx, dxp, dyp, dy, carry, ops, prefix, pops, pprefix;
+    std::vector<Request*> reqs;
+    std::vector<long long> off;
+    std::vector<int> mats;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct mr_server {
+    mr_server_config cfg{};
+    std::mutex mu;
+    std::condition_variable cv_sched, cv_done, cv_lane;
+    std::vector<Matrix> mats;
+    std::deque<Request*> pending;
+    std::unordered_map<uint64_t, Request*> reqs;
+    std::vector<Lane> lanes;
+    std::deque<int> inflight;  // lane indices in launch order
+    uint64_t next_ticket = 1;
+    uint64_t use_clock = 0;
+    size_t resident_bytes = 0;
+    bool stop = false;
+    std::thread sched, compl_;
+    cudaStream_t admit_st = nullptr;
+    int device = 0;
+    // stats
+    std::vector<double> lat;
+    int64_t submitted = 0, completed = 0, batches = 0, admissions = 0, evictions = 0, rejected = 0, batch_items = 0;
+    Clock::time_point t_first{}, t_last{};
+    bool have_first = false;
+};
+
+namespace {
+
+size_t matrix_bytes(const Matrix& m)
+{
+    const int64_t items = (int64_t)m.n + m.nnz;
+    const int64_t lanes = (items + 13) / 14;
+    const int64_t tiles = (lanes + 31) / 32;
+    return sizeof(int32_t) * ((size_t)m.n + 1) + (sizeof(int32_t) + dtype_size(m.dtype)) * (size_t)m.nnz +
+           (m.h_perm ? sizeof(int32_t) * (size_t)m.n : 0) + 4 * (size_t)lanes + 8 * (size_t)(tiles + 1) + 1024;
+}
+
+void free_resident(Matrix& m, cudaStream_t st)
+{
+    cudaFreeAsync(m.d_rowptr, st);
+    cudaFreeAsync(m.d_colidx, st);
+    cudaFreeAsync(m.d_vals, st);
+    if (m.d_perm) cudaFreeAsync(m.d_perm, st);
+    cudaFreeAsync(m.plan.tile_x, st);
+    cudaFreeAsync(m.plan.tile_y, st);
+    cudaFreeAsync(m.plan.lane_desc, st);
+    m.d_rowptr = m.d_colidx = m.d_perm = nullptr;
+    m.d_vals = nullptr;
+    m.plan.tile_x = m.plan.tile_y = nullptr;
+    m.plan.lane_desc = nullptr;
+    m.resident = false;
+}
+
+// upload + plan on the admission stream (called with the server lock held)
+int make_resident(mr_server* s, Matrix& m)
+{
+    cudaStream_t st = s->admit_st;
+    const size_t vb = dtype_size(m.dtype);
+    auto alloc = [&](void** p, size_t b) { return cudaMallocAsync(p, std::max<size_t>(b, 16), st) == cudaSuccess; };
+    m.plan = MerbitPlan();
+    m.plan.sigma = s->cfg.sigma;
+    m.plan.block = 256;
+    m.plan.n_rows = m.n;
+    m.plan.nnz = m.nnz;
+    const int64_t items = (int64_t)m.n + m.nnz;
+    m.plan.lane_num = (int)((items + m.plan.sigma - 1) / m.plan.sigma);
+    m.plan.tile_num = (m.plan.lane_num + 31) / 32;
+    const size_t desc_b = m.plan.sigma < 15 ? 4 : 8;
+    bool ok = alloc((void**)&m.d_rowptr, 4 * ((size_t)m.n + 1)) && alloc((void**)&m.d_colidx, 4 * (size_t)m.nnz) &&
+              alloc(&m.d_vals, vb * (size_t)m.nnz) && (!m.h_perm || alloc((void**)&m.d_perm, 4 * (size_t)m.n)) &&
+              alloc((void**)&m.plan.tile_x, 4 * ((size_t)m.plan.tile_num + 1)) &&
+              alloc((void**)&m.plan.tile_y, 4 * ((size_t)m.plan.tile_num + 1)) &&
+              alloc(&m.plan.lane_desc, desc_b * (size_t)std::max(m.plan.lane_num, 1));
+    if (!ok) {
+        cudaGetLastError();
+        free_resident(m, st);
+        return MR_ERR_NOMEM;
+    }
+    cudaMemcpyAsync(m.d_rowptr, m.h_rowptr, 4 * ((size_t)m.n + 1), cudaMemcpyHostToDevice, st);
+    if (m.nnz > 0) {
+        cudaMemcpyAsync(m.d_colidx, m.h_colidx, 4 * (size_t)m.nnz, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(m.d_vals, m.h_vals, vb * (size_t)m.nnz, cudaMemcpyHostToDevice, st);
+    }
+    if (m.h_perm) cudaMemcpyAsync(m.d_perm, m.h_perm, 4 * (size_t)m.n, cudaMemcpyHostToDevice, st);
+    int rc = launch_merbit_plan(m.d_rowptr, m.n, (int)m.nnz, m.plan.sigma, m.plan.lane_num, m.plan.tile_num,
+                                m.plan.tile_x, m.plan.tile_y, m.plan.lane_desc, st);
+    if (rc == MR_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = MR_ERR_CUDA;
+    if (rc != MR_OK) {
+        free_resident(m, st);
+        return rc;
+    }
+    m.resident = true;
+    m.bytes = matrix_bytes(m);
+    return MR_OK;
+}
+
+// make room for `need` bytes by evicting least recently used idle matrices
+bool make_room(mr_server* s, size_t need, const std::vector<int>& keep)
+{
+    while (s->resident_bytes + need > (size_t)s->cfg.hbm_budget_bytes) {
+        int victim = -1;
+        for (int i = 0; i < (int)s->mats.size(); ++i) {
+            const Matrix& m = s->mats[(size_t)i];
+            if (!m.resident || m.refs > 0) continue;
+            if (std::find(keep.begin(), keep.end(), i) != keep.end()) continue;
+            if (victim < 0 || m.last_use < s->mats[(size_t)victim].last_use) victim = i;
+        }
+        if (victim < 0) return false;
+        Matrix& v = s->mats[(size_t)victim];
+        free_resident(v, s->admit_st);
+        s->resident_bytes -= v.bytes;
+        ++s->evictions;
+    }
+    return true;
+}
+
+int launch_batch(mr_server* s, Lane& L)
+{
+    const int count = (int)L.reqs.size();
+    L.off.assign((size_t)count + 1, 0);
+    for (int i = 0; i < count; ++i) L.off[(size_t)i + 1] = L.off[(size_t)i] + s->mats[(size_t)L.mats[(size_t)i]].n;
+    const long long total = L.off[(size_t)count];
+    MR_TRY(L.hx.reserve((size_t)total + 1));
+    MR_TRY(L.hy.reserve((size_t)total + 1));
+    for (int i = 0; i < count; ++i)
+        std::memcpy(L.hx.p + L.off[(size_t)i], L.reqs[(size_t)i]->x, sizeof(float) * (size_t)(L.off[(size_t)i + 1] - L.off[(size_t)i]));
+    const size_t vbytes = sizeof(float) * (size_t)(total + 1);
+    MR_TRY(L.dx.reserve(vbytes, L.st));
+    MR_TRY(L.dxp.reserve(vbytes, L.st));
+    MR_TRY(L.dyp.reserve(vbytes, L.st));
+    MR_TRY(L.dy.reserve(vbytes, L.st));
+    // group the items by (sigma, dtype): one batched kernel per group
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    long long carry_total = 0;
+    std::vector<long long> carry_off((size_t)count);
+    for (int i = 0; i < count; ++i) {
+        const Matrix& m = s->mats[(size_t)L.mats[(size_t)i]];
+        groups[{m.plan.sigma, m.dtype}].push_back(i);
+        carry_off[(size_t)i] = carry_total;
+        carry_total += std::max(m.plan.tile_num, 1);
+    }
+    MR_TRY(L.carry.reserve(sizeof(float) * (size_t)carry_total, L.st));
+    size_t ops_bytes = 0;
+    for (auto& g : groups) ops_bytes += batch_op_bytes(g.first.second, g.first.first) * g.second.size() + 256;
+    MR_TRY(L.ops.reserve(ops_bytes, L.st));
+    MR_TRY(L.prefix.reserve(sizeof(long long) * ((size_t)count + groups.size() * 2 + 2), L.st));
+    MR_TRY(L.pops.reserve(sizeof(PermOp) * (size_t)count, L.st));
+    MR_TRY(L.pprefix.reserve(sizeof(long long) * ((size_t)count + 1), L.st));
+    // host tables, copied with the vectors (pinned staging after the y area)
+    std::vector<unsigned char> ops_host(ops_bytes);
+    std::vector<long long> prefix_host;
+    std::vector<PermOp> pops((size_t)count);
+    float* dx = static_cast<float*>(L.dx.p);
+    float* dxp = static_cast<float*>(L.dxp.p);
+    float* dyp = static_cast<float*>(L.dyp.p);
+    float* dy = static_cast<float*>(L.dy.p);
+    float* carry = static_cast<float*>(L.carry.p);
+    struct GroupLaunch {
+        int dtype, sigma, count;
+        size_t ops_at, prefix_at;
+        long long tiles;
+    };
+    std::vector<GroupLaunch> gl;
+    size_t at = 0;
+    for (auto& g : groups) {
+        const int sigma = g.first.first, dtype = g.first.second;
+        const size_t ob = batch_op_bytes(dtype, sigma);
+        GroupLaunch x{dtype, sigma, (int)g.second.size(), at, prefix_host.size(), 0};
+        prefix_host.push_back(0);
+        for (int i : g.second) {
+            const Matrix& m = s->mats[(size_t)L.mats[(size_t)i]];
+            const mr_csr_view A{m.n, m.n, m.nnz, m.d_rowptr, m.d_colidx, m.d_vals, m.dtype};
+            MR_TRY(batch_fill_op(ops_host.data() + at, dtype, sigma, m.plan, A, dxp + L.off[(size_t)i],
+                                 dyp + L.off[(size_t)i], carry + carry_off[(size_t)i]));
+            at += ob;
+            x.tiles += m.plan.tile_num;
+            prefix_host.push_back(x.tiles);
+        }
+        at = (at + 255) / 256 * 256;
+        gl.push_back(x);
+    }
+    for (int i = 0; i < count; ++i) {
+        const Matrix& m = s->mats[(size_t)L.mats[(size_t)i]];
+        pops[(size_t)i] = PermOp{m.d_perm, L.off[(size_t)i], m.n};
+    }
+    cudaStream_t st = L.st;
+    MR_CUDA_TRY(cudaMemcpyAsync(dx, L.hx.p, sizeof(float) * (size_t)total, cudaMemcpyHostToDevice, st));
+    // the small tables go through pageable memory; the copy is synchronous
+    // with respect to the host buffer, which is then free to reuse
+    MR_CUDA_TRY(cudaMemcpyAsync(L.ops.p, ops_host.data(), at, cudaMemcpyHostToDevice, st));
+    MR_CUDA_TRY(cudaMemcpyAsync(L.prefix.p, prefix_host.data(), sizeof(long long) * prefix_host.size(),
+                                cudaMemcpyHostToDevice, st));
+    MR_CUDA_TRY(cudaMemcpyAsync(L.pops.p, pops.data(), sizeof(PermOp) * (size_t)count, cudaMemcpyHostToDevice, st));
+    MR_CUDA_TRY(cudaMemcpyAsync(L.pprefix.p, L.off.data(), sizeof(long long) * (size_t)count, cudaMemcpyHostToDevice,
+                                st));
+    const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 8));
+    const PermOp* d_pops = static_cast<const PermOp*>(L.pops.p);
+    const long long* d_pprefix = static_cast<const long long*>(L.pprefix.p);
+    batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dx, dxp, 0);
+    MR_CUDA_TRY(cudaGetLastError());
+    for (const auto& g : gl)
+        MR_TRY(batch_launch_ops(g.dtype, g.sigma, static_cast<unsigned char*>(L.ops.p) + g.ops_at,
+                                static_cast<const long long*>(L.prefix.p) + g.prefix_at, g.count, g.tiles, st));
+    batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
+    MR_CUDA_TRY(cudaGetLastError());
+    MR_CUDA_TRY(cudaMemcpyAsync(L.hy.p, dy, sizeof(float) * (size_t)total, cudaMemcpyDeviceToHost, st));
+    MR_CUDA_TRY(cudaEventRecord(L.done, st));
+    return MR_OK;
+}
+
+void finish_requests(mr_server* s, std::vector<Request*>& rs, int status)
+{
+    const auto now = Clock::now();
+    for (Request* r : rs) {
+        r->status = status;
+        r->latency_us = std::chrono::duration<double, std::micro>(now - r->t_submit).count();
+        r->done = true;
+        if (status == MR_OK) {
+            s->lat.push_back(r->latency_us);
+            ++s->completed;
+        } else {
+            ++s->rejected;
+        }
+    }
+    s->t_last = now;
+}
+
+void scheduler_loop(mr_server* s)
+{
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv_sched.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+        if (s->stop) return;
+        // batching window: from the first pending request's arrival
+        const auto deadline = s->pending.front()->t_submit + std::chrono::microseconds(s->cfg.window_us);
+        s->cv_sched.wait_until(lk, deadline, [&] { return s->stop || (int)s->pending.size() >= s->cfg.max_batch; });
+        if (s->stop) return;
+        int lane = -1;
+        s->cv_lane.wait(lk, [&] {
+            if (s->stop) return true;
+            for (int i = 0; i < (int)s->lanes.size(); ++i)
+                if (!s->lanes[(size_t)i].busy) {
+                    lane = i;
+                    return true;
+                }
+            return false;
+        });
+        if (s->stop) return;
+        Lane& L = s->lanes[(size_t)lane];
+        L.reqs.clear();
+        L.mats.clear();
+        std::vector<int> keep;
+        std::deque<Request*> deferred;
+        while (!s->pending.empty() && (int)L.reqs.size() < s->cfg.max_batch) {
+            Request* r = s->pending.front();
+            s->pending.pop_front();
+            Matrix& m = s->mats[(size_t)r->id];
+            if (!m.resident) {
+                const size_t need = matrix_bytes(m);
+                if (need > (size_t)s->cfg.hbm_budget_bytes) {  // can never fit
+                    std::vector<Request*> one{r};
+                    finish_requests(s, one, MR_ERR_BUSY);
+                    continue;
+                }
+                if (!make_room(s, need, keep)) {  // all room is pinned by batches in flight
+                    deferred.push_back(r);
+                    continue;
+                }
+                const int rc = make_resident(s, m);
+                if (rc != MR_OK) {
+                    std::vector<Request*> one{r};
+                    finish_requests(s, one, rc);
+                    continue;
+                }
+                s->resident_bytes += m.bytes;
+                ++s->admissions;
+            }
+            m.last_use = ++s->use_clock;
+            ++m.refs;
+            keep.push_back(r->id);
+            L.reqs.push_back(r);
+            L.mats.push_back(r->id);
+        }
+        for (auto it = deferred.rbegin(); it != deferred.rend(); ++it) s->pending.push_front(*it);
+        if (L.reqs.empty()) {
+            // everything deferred: wait for a batch to finish and free room
+            s->cv_done.wait_for(lk, std::chrono::milliseconds(1));
+            continue;
+        }
+        L.busy = true;
+        const int rc = launch_batch(s, L);
+        if (rc != MR_OK) {
+            for (int id : L.mats) --s->mats[(size_t)id].refs;
+            finish_requests(s, L.reqs, rc);
+            L.busy = false;
+            s->cv_done.notify_all();
+            continue;
+        }
+        ++s->batches;
+        s->batch_items += (int64_t)L.reqs.size();
+        s->inflight.push_back(lane);
+        s->cv_done.notify_all();  // wakes the completion thread
+    }
+}
+
+void completion_loop(mr_server* s)
+{
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv_done.wait(lk, [&] { return s->stop || !s->inflight.empty(); });
+        if (s->inflight.empty() && s->stop) return;
+        const int lane = s->inflight.front();
+        Lane& L = s->lanes[(size_t)lane];
+        lk.unlock();
+        const cudaError_t e = cudaEventSynchronize(L.done);
+        // results to the callers' buffers
+        if (e == cudaSuccess)
+            for (size_t i = 0; i < L.reqs.size(); ++i)
+                std::memcpy(L.reqs[i]->y, L.hy.p + L.off[i], sizeof(float) * (size_t)(L.off[i + 1] - L.off[i]));
+        lk.lock();
+        s->inflight.pop_front();
+        for (int id : L.mats) --s->mats[(size_t)id].refs;
+        finish_requests(s, L.reqs, e == cudaSuccess ? MR_OK : MR_ERR_CUDA);
+        L.reqs.clear();
+        L.busy = false;
+        s->cv_done.notify_all();
+        s->cv_lane.notify_all();
+        s->cv_sched.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mr_server_create(const mr_server_config* cfg, mr_server** out)
+{
+    if (!out) return MR_ERR_INVALID_ARG;
+    *out = nullptr;
+    auto* s = new (std::nothrow) mr_server;
+    if (!s) return MR_ERR_NOMEM;
+    if (cfg) s->cfg = *cfg;
+    if (s->cfg.window_us <= 0) s->cfg.window_us = 200;
+    if (s->cfg.max_batch <= 0) s->cfg.max_batch = 256;
+    if (s->cfg.lanes <= 0) s->cfg.lanes = 3;
+    if (s->cfg.sigma <= 0) s->cfg.sigma = 14;
+    if (!merbit_sigma_supported(s->cfg.sigma) || s->cfg.lanes > 16) {
+        delete s;
+        return MR_ERR_INVALID_ARG;
+    }
+    cudaGetDevice(&s->device);
+    if (s->cfg.hbm_budget_bytes <= 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        s->cfg.hbm_budget_bytes = (int64_t)(fr / 2);
+    }
+    s->lanes.resize((size_t)s->cfg.lanes);
+    bool ok = cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) == cudaSuccess;
+    for (auto& L : s->lanes)
+        ok = ok && cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        mr_server_destroy(s);
+        return MR_ERR_CUDA;
+    }
+    s->sched = std::thread(scheduler_loop, s);
+    s->compl_ = std::thread(completion_loop, s);
+    *out = s;
+    return MR_OK;
+}
+
+int mr_server_add_matrix(mr_server* s, int32_t n, int64_t nnz, const int32_t* rowptr, const int32_t* colidx,
+                         const void* vals, int32_t dtype, const int32_t* perm_old2new, int32_t* id)
+{
+    if (!s || !id || n <= 0 || nnz < 0 || nnz > INT32_MAX || !rowptr || (nnz > 0 && (!colidx || !vals)))
+        return MR_ERR_INVALID_ARG;
+    if (dtype != MR_F32 && dtype != MR_F16 && dtype != MR_BF16) return MR_ERR_UNSUPPORTED;
+    // host-side validation (the pool admits matrices without a device check)
+    if (rowptr[0] != 0 || rowptr[n] != nnz) return MR_ERR_INVALID_ARG;
+    for (int32_t i = 0; i < n; ++i)
+        if (rowptr[i + 1] < rowptr[i]) return MR_ERR_INVALID_ARG;
+    for (int64_t k = 0; k < nnz; ++k)
+        if (colidx[k] < 0 || colidx[k] >= n) return MR_ERR_INVALID_ARG;
+    if (perm_old2new) {
+        std::vector<char> seen((size_t)n, 0);
+        for (int32_t i = 0; i < n; ++i) {
+            const int32_t p = perm_old2new[i];
+            if (p < 0 || p >= n || seen[(size_t)p]) return MR_ERR_INVALID_PERM;
+            seen[(size_t)p] = 1;
+        }
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    Matrix m;
+    m.n = n;
+    m.nnz = nnz;
+    m.dtype = dtype;
+    m.h_rowptr = rowptr;
+    m.h_colidx = colidx;
+    m.h_vals = vals;
+    m.h_perm = perm_old2new;
+    s->mats.push_back(m);
+    *id = (int32_t)s->mats.size() - 1;
+    return MR_OK;
+}
+
+int mr_server_submit(mr_server* s, int32_t id, const float* x, float* y, uint64_t* ticket)
+{
+    if (!s || !x || !y) return MR_ERR_INVALID_ARG;
+    auto* r = new (std::nothrow) Request;
+    if (!r) return MR_ERR_NOMEM;
+    r->id = id;
+    r->x = x;
+    r->y = y;
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (id < 0 || id >= (int)s->mats.size()) {
+            delete r;
+            return MR_ERR_NOT_FOUND;
+        }
+        r->ticket = s->next_ticket++;
+        s->reqs[r->ticket] = r;
+        s->pending.push_back(r);
+        ++s->submitted;
+        if (!s->have_first) {
+            s->t_first = r->t_submit;
+            s->have_first = true;
+        }
+    }
+    s->cv_sched.notify_one();
+    if (ticket) *ticket = r->ticket;
+    return MR_OK;
+}
+
+int mr_server_wait(mr_server* s, uint64_t ticket, int32_t timeout_ms, double* latency_us)
+{
+    if (!s) return MR_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return MR_ERR_NOT_FOUND;
+    Request* r = it->second;
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms),
+                                        [&] { return r->done; });
+    if (!ok) return MR_ERR_TIMEOUT;
+    const int st = r->status;
+    if (latency_us) *latency_us = r->latency_us;
+    s->reqs.erase(it);
+    delete r;
+    return st;
+}
+
+int mr_server_drain(mr_server* s, int32_t timeout_ms)
+{
+    if (!s) return MR_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    const bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms), [&] {
+        return s->pending.empty() && s->inflight.empty() && s->completed + s->rejected == s->submitted;
+    });
+    // forget finished requests nobody waits for
+    for (auto it = s->reqs.begin(); it != s->reqs.end();) {
+        if (it->second->done) {
+            delete it->second;
+            it = s->reqs.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    return ok ? MR_OK : MR_ERR_TIMEOUT;
+}
+
+int mr_server_get_stats(mr_server* s, mr_server_stats* out)
+{
+    if (!s || !out) return MR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    mr_server_stats st{};
+    st.submitted = s->submitted;
+    st.completed = s->completed;
+    st.rejected = s->rejected;
+    st.batches = s->batches;
+    st.admissions = s->admissions;
+    st.evictions = s->evictions;
+    st.resident_bytes = (int64_t)s->resident_bytes;
+    int64_t nres = 0;
+    for (const auto& m : s->mats) nres += m.resident ? 1 : 0;
+    st.resident_matrices = nres;
+    st.mean_batch = s->batches ? (double)s->batch_items / (double)s->batches : 0.0;
+    if (!s->lat.empty()) {
+        std::vector<double> v = s->lat;
+        auto pct = [&](double q) {
+            const size_t k = std::min(v.size() - 1, (size_t)(q * (double)(v.size() - 1) + 0.5));
+            std::nth_element(v.begin(), v.begin() + (long)k, v.end());
+            return v[k];
+        };
+        st.p50_us = pct(0.50);
+        st.p99_us = pct(0.99);
+        double sum = 0, mx = 0;
+        for (double d : s->lat) {
+            sum += d;
+            mx = std::max(mx, d);
+        }
+        st.mean_us = sum / (double)s->lat.size();
+        st.max_us = mx;
+        const double span = std::chrono::duration<double>(s->t_last - s->t_first).count();
+        st.req_per_s = span > 0 ? (double)s->completed / span : 0.0;
+    }
+    *out = st;
+    return MR_OK;
+}
+
+int mr_server_reset_stats(mr_server* s)
+{
+    if (!s) return MR_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->lat.clear();
+    s->submitted -= s->completed + s->rejected;
+    s->completed = s->rejected = s->batches = s->batch_items = 0;
+    s->admissions = s->evictions = 0;
+    s->have_first = false;
+    return MR_OK;
+}
+
+int mr_server_destroy(mr_server* s)
+{
+    if (!s) return MR_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_sched.notify_all();
+    s->cv_lane.notify_all();
+    s->cv_done.notify_all();
+    if (s->sched.joinable()) s->sched.join();
+    if (s->compl_.joinable()) s->compl_.join();
+    cudaDeviceSynchronize();
+    for (auto& m : s->mats)
+        if (m.resident) free_resident(m, s->admit_st);
+    for (auto& L : s->lanes) {
+        for (DevVec* d : {&L.dx, &L.dxp, &L.dyp, &L.dy, &L.carry, &L.ops, &L.prefix, &L.pops, &L.pprefix})
+            if (d->p) cudaFreeAsync(d->p, s->admit_st);
+        if (L.done) cudaEventDestroy(L.done);
+        if (L.st) cudaStreamDestroy(L.st);
+    }
+    if (s->admit_st) {
+        cudaStreamSynchronize(s->admit_st);
+        cudaStreamDestroy(s->admit_st);
+    }
+    for (auto& kv : s->reqs) delete kv.second;
+    for (Request* r : s->pending)
+        if (s->reqs.find(r->ticket) == s->reqs.end()) delete r;
+    delete s;
+    return MR_OK;
+}
+
+// Open-loop Poisson load: n_requests arrivals at `rate` per second, matrix
+// ids drawn uniformly from ids[], x / y buffers per id (y buffers are
+// overwritten by every request of that id). Returns after all completed.
+int mr_server_loadgen(mr_server* s, const int32_t* ids, int32_t n_ids, int64_t n_requests, double rate,
+                      uint64_t seed, const float* const* x_of, float* const* y_of, int32_t timeout_ms)
+{
+    if (!s || !ids || n_ids <= 0 || n_requests < 0 || rate <= 0 || !x_of || !y_of) return MR_ERR_INVALID_ARG;
+    std::mt19937_64 rng(seed);
+    std::exponential_distribution<double> gap(rate);
+    std::uniform_int_distribution<int> pick(0, n_ids - 1);
+    auto t = Clock::now();
+    for (int64_t i = 0; i < n_requests; ++i) {
+        t += std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(gap(rng)));
+        while (Clock::now() < t) {
+            // spin: arrivals are tens of microseconds apart
+        }
+        const int k = pick(rng);
+        MR_TRY(mr_server_submit(s, ids[k], x_of[k], y_of[k], nullptr));
+    }
+    return mr_server_drain(s, timeout_ms);
+}
+
+}  // extern "C"

@@ -52,7 +52,8 @@ class CsrView(C.Structure):
 class PlanInfo(C.Structure):
     _fields_ = [("sigma", C.c_int32), ("block", C.c_int32), ("n_rows", C.c_int32), ("nnz", C.c_int64),
                 ("lane_num", C.c_int32), ("tile_num", C.c_int32), ("desc_bytes", C.c_int32),
-                ("tile_x_dev", C.c_void_p), ("tile_y_dev", C.c_void_p), ("lane_desc_dev", C.c_void_p)]
+                ("tile_x_dev", C.c_void_p), ("tile_y_dev", C.c_void_p), ("lane_desc_dev", C.c_void_p),
+                ("hub_columns", C.c_int32), ("hub_coverage", C.c_double)]
 
 
 _lib = None
@@ -79,6 +80,7 @@ def lib():
     _sig(L.mr_version, C.c_int)
     _sig(L.mr_spmv_csr, C.c_int, P(CsrView), vp, vp, vp)
     _sig(L.mr_merbit_plan_create, C.c_int, P(CsrView), C.c_int, C.c_int, vp, P(vp))
+    _sig(L.mr_merbit_plan_create_ex, C.c_int, P(CsrView), C.c_int, C.c_int, C.c_int, vp, P(vp))
     _sig(L.mr_merbit_plan_destroy, C.c_int, vp)
     _sig(L.mr_merbit_plan_get_info, C.c_int, vp, P(PlanInfo))
     _sig(L.mr_spmv_merbit, C.c_int, vp, P(CsrView), vp, vp, vp)
@@ -151,10 +153,10 @@ def spmv_csr(A: CsrView, x, y, stream=None) -> None:
 class MerbitPlan:
     """Owner of an mr_merbit_plan (the reference's TILE<BLOCK,SIGMA>)."""
 
-    def __init__(self, A: CsrView, sigma: int = 14, block: int = 0, stream=None):
+    def __init__(self, A: CsrView, sigma: int = 14, block: int = 0, stream=None, hub_cache: bool = True):
         h = C.c_void_p()
-        check(lib().mr_merbit_plan_create(C.byref(A), sigma, block, _stream(stream), C.byref(h)),
-              "mr_merbit_plan_create")
+        check(lib().mr_merbit_plan_create_ex(C.byref(A), sigma, block, 0 if hub_cache else 1, _stream(stream),
+                                             C.byref(h)), "mr_merbit_plan_create_ex")
         self.h = h
         self.A = A
 
@@ -456,10 +458,10 @@ def _batch_sigs(L):
     _sig(L.mr_batch_set_vectors, C.c_int, vp, i32, vp, vp, vp)
     _sig(L.mr_batch_info, C.c_int, vp, P(i32), P(i64))
     _sig(L.mr_batch_destroy, C.c_int, vp)
-    _sig(L.mr_autotune_merbit, C.c_int, P(CsrView), vp, vp, i32, P(i32), P(i32), P(C.c_float), vp)
+    _sig(L.mr_autotune_merbit, C.c_int, P(CsrView), vp, vp, i32, P(i32), P(i32), P(i32), P(C.c_float), vp)
     _sig(L.mr_tuner_create, C.c_int, P(vp))
     _sig(L.mr_tuner_destroy, C.c_int, vp)
-    _sig(L.mr_tuner_pick, C.c_int, vp, P(CsrView), vp, vp, P(i32), P(i32), vp)
+    _sig(L.mr_tuner_pick, C.c_int, vp, P(CsrView), vp, vp, P(i32), P(i32), P(i32), vp)
     _sig(L.mr_tuner_stats, C.c_int, vp, P(i32), P(i32))
     L._batch_sigs = True
 
@@ -512,10 +514,10 @@ class Batch:
 def autotune(A: CsrView, x, y, reps: int = 5, stream=None):
     L = lib()
     _batch_sigs(L)
-    s, b, ms = C.c_int32(0), C.c_int32(0), C.c_float(0)
-    check(L.mr_autotune_merbit(C.byref(A), _ptr(x), _ptr(y), reps, C.byref(s), C.byref(b), C.byref(ms),
+    s, b, f, ms = C.c_int32(0), C.c_int32(0), C.c_int32(0), C.c_float(0)
+    check(L.mr_autotune_merbit(C.byref(A), _ptr(x), _ptr(y), reps, C.byref(s), C.byref(b), C.byref(f), C.byref(ms),
                                _stream(stream)), "mr_autotune_merbit")
-    return s.value, b.value, ms.value
+    return s.value, b.value, f.value, ms.value
 
 
 class Tuner:
@@ -527,10 +529,10 @@ class Tuner:
         self.h = h
 
     def pick(self, A: CsrView, x, y, stream=None):
-        s, b = C.c_int32(0), C.c_int32(0)
-        check(lib().mr_tuner_pick(self.h, C.byref(A), _ptr(x), _ptr(y), C.byref(s), C.byref(b), _stream(stream)),
-              "mr_tuner_pick")
-        return s.value, b.value
+        s, b, f = C.c_int32(0), C.c_int32(0), C.c_int32(0)
+        check(lib().mr_tuner_pick(self.h, C.byref(A), _ptr(x), _ptr(y), C.byref(s), C.byref(b), C.byref(f),
+                                  _stream(stream)), "mr_tuner_pick")
+        return s.value, b.value, f.value
 
     def stats(self):
         a, b = C.c_int32(0), C.c_int32(0)
@@ -540,6 +542,114 @@ class Tuner:
     def close(self):
         if getattr(self, "h", None):
             lib().mr_tuner_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- serving ----
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("window_us", C.c_int32), ("max_batch", C.c_int32),
+                ("lanes", C.c_int32), ("sigma", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("rejected", C.c_int64),
+                ("batches", C.c_int64), ("admissions", C.c_int64), ("evictions", C.c_int64),
+                ("resident_bytes", C.c_int64), ("resident_matrices", C.c_int64), ("mean_batch", C.c_double),
+                ("p50_us", C.c_double), ("p99_us", C.c_double), ("mean_us", C.c_double), ("max_us", C.c_double),
+                ("req_per_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _server_sigs(L):
+    if getattr(L, "_server_sigs", False):
+        return
+    vp, i32, i64, u64 = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64
+    P = C.POINTER
+    _sig(L.mr_server_create, C.c_int, P(ServerConfig), P(vp))
+    _sig(L.mr_server_add_matrix, C.c_int, vp, i32, i64, vp, vp, vp, i32, vp, P(i32))
+    _sig(L.mr_server_submit, C.c_int, vp, i32, vp, vp, P(u64))
+    _sig(L.mr_server_wait, C.c_int, vp, u64, i32, P(C.c_double))
+    _sig(L.mr_server_drain, C.c_int, vp, i32)
+    _sig(L.mr_server_get_stats, C.c_int, vp, P(ServerStats))
+    _sig(L.mr_server_reset_stats, C.c_int, vp)
+    _sig(L.mr_server_destroy, C.c_int, vp)
+    _sig(L.mr_server_loadgen, C.c_int, vp, vp, i32, i64, C.c_double, u64, vp, vp, i32)
+    L._server_sigs = True
+
+
+class Server:
+    """mr_server: continuous-batching SpMV over a device-resident pool.
+    Host arrays passed to add_matrix / submit are kept referenced here for
+    as long as the server may read or write them."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, window_us: int = 200, max_batch: int = 256, lanes: int = 3,
+                 sigma: int = 14):
+        L = lib()
+        _server_sigs(L)
+        cfg = ServerConfig(hbm_budget_bytes, window_us, max_batch, lanes, sigma)
+        h = C.c_void_p()
+        check(L.mr_server_create(C.byref(cfg), C.byref(h)), "mr_server_create")
+        self.h = h
+        self._keep = []
+
+    def add_matrix(self, rowptr, colidx, vals, perm_old2new=None) -> int:
+        rowptr = np.ascontiguousarray(rowptr, np.int32)
+        colidx = np.ascontiguousarray(colidx, np.int32)
+        if vals.dtype == np.float32:
+            dt = MR_F32
+        elif vals.dtype == np.float16:
+            dt = MR_F16
+        else:
+            raise ValueError("vals must be float32 or float16")
+        vals = np.ascontiguousarray(vals)
+        perm = None if perm_old2new is None else np.ascontiguousarray(perm_old2new, np.int32)
+        self._keep.append((rowptr, colidx, vals, perm))
+        i = C.c_int32(0)
+        check(lib().mr_server_add_matrix(self.h, rowptr.size - 1, colidx.size, rowptr.ctypes.data, colidx.ctypes.data,
+                                         vals.ctypes.data, dt, None if perm is None else perm.ctypes.data,
+                                         C.byref(i)), "mr_server_add_matrix")
+        return i.value
+
+    def submit(self, mid: int, x: np.ndarray, y: np.ndarray) -> int:
+        t = C.c_uint64(0)
+        check(lib().mr_server_submit(self.h, mid, x.ctypes.data, y.ctypes.data, C.byref(t)), "mr_server_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 10000):
+        lat = C.c_double(0)
+        rc = lib().mr_server_wait(self.h, ticket, timeout_ms, C.byref(lat))
+        return rc, lat.value
+
+    def drain(self, timeout_ms: int = 60000):
+        check(lib().mr_server_drain(self.h, timeout_ms), "mr_server_drain")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib().mr_server_get_stats(self.h, C.byref(st)), "mr_server_get_stats")
+        return st.as_dict()
+
+    def reset_stats(self):
+        check(lib().mr_server_reset_stats(self.h), "mr_server_reset_stats")
+
+    def loadgen(self, ids, xs, ys, n_requests: int, rate: float, seed: int = 1, timeout_ms: int = 600000):
+        ids_a = np.ascontiguousarray(ids, np.int32)
+        xp = (C.c_void_p * len(xs))(*[a.ctypes.data for a in xs])
+        yp = (C.c_void_p * len(ys))(*[a.ctypes.data for a in ys])
+        check(lib().mr_server_loadgen(self.h, ids_a.ctypes.data, ids_a.size, n_requests, rate, seed, xp, yp,
+                                      timeout_ms), "mr_server_loadgen")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mr_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

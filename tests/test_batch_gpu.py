@@ -121,8 +121,8 @@ def test_autotuner(M):
     A = M.view(_dev(rp), _dev(ci), _dev(v))
     x = _dev(M.uniform(rp.size - 1, seed=1))
     y = torch.empty_like(x)
-    s, b, ms = M.autotune(A, x, y, reps=3)
-    assert s in (7, 10, 14, 16, 20, 24, 28, 32) and b in (128, 256, 512) and ms > 0
+    s, b, f, ms = M.autotune(A, x, y, reps=3)
+    assert s in (7, 10, 14, 16, 20, 24, 28, 32) and b in (128, 256, 512, 1024) and f in (0, 1) and ms > 0
     t = M.Tuner()
     assert t.pick(A, x, y) == t.pick(A, x, y)
     assert t.stats() == (1, 1)

@@ -1,0 +1,122 @@
+"""Serving loop: continuous batching over a device-resident pool.
+
+Each result must match the FP64 oracle of the stored values (within the
+FP32-accumulation tolerance), be bitwise identical alone and in a mixed
+batch, survive LRU eviction under a tight HBM budget, and report
+admission refusals, timeouts and latency statistics."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _pool(M):
+    mats = []
+    specs = [("rmat", 12, 16), ("band", 20000, 17), ("rmat", 14, 8), ("band", 3000, 3), ("rmat", 13, 24)]
+    for i, (kind, a, b) in enumerate(specs):
+        if kind == "rmat":
+            rp, ci, v = M.gen_rmat(scale=a, edge_factor=b, seed=i + 1)
+        else:
+            rp, ci, v = M.gen_banded(a, b, seed=i + 1)
+        n2o = M.pgorder(rp, ci, 0, 5)
+        perm = np.empty(rp.size - 1, np.int32)
+        perm[n2o] = np.arange(rp.size - 1, dtype=np.int32)
+        # the pool holds the reordered matrix and its permutation
+        import pyoracle as O
+        brp, bci, bv = O.permute_csr(rp, ci, v, perm)
+        mats.append(dict(orig=(rp, ci, v), reordered=(brp, bci, bv), perm=perm))
+    return mats
+
+
+@pytest.fixture(scope="module")
+def pool(M):
+    return _pool(M)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float16])
+def test_results_match_fp64_and_are_identical_alone_and_mixed(M, O, pool, dtype):
+    srv = M.Server(window_us=300, max_batch=64, lanes=3)
+    ids = []
+    for m in pool:
+        brp, bci, bv = m["reordered"]
+        ids.append(srv.add_matrix(brp, bci, bv.astype(dtype), m["perm"]))
+    rng = np.random.default_rng(0)
+    reqs = []
+    for k in range(24):
+        j = int(rng.integers(0, len(pool)))
+        n = pool[j]["perm"].size
+        reqs.append((j, M.uniform(n, seed=100 + k)))
+    # alone: one request at a time
+    alone = []
+    for j, x in reqs:
+        y = np.full(x.size, np.nan, np.float32)
+        rc, lat = srv.wait(srv.submit(ids[j], x, y))
+        assert rc == M.MR_OK and lat > 0
+        alone.append(y)
+    # mixed: all at once, batched together
+    ys = [np.full(x.size, np.nan, np.float32) for _, x in reqs]
+    tickets = [srv.submit(ids[j], x, y) for (j, x), y in zip(reqs, ys)]
+    for t in tickets:
+        assert srv.wait(t)[0] == M.MR_OK
+    for (j, x), ya, ym in zip(reqs, alone, ys):
+        assert np.array_equal(ya.view(np.int32), ym.view(np.int32))
+        rp, ci, v = pool[j]["orig"]
+        vr = v.astype(dtype).astype(np.float32)
+        assert _rel(ym, O.spmv_f64(rp, ci, vr, x)) <= 1e-5
+    st = srv.stats()
+    assert st["completed"] == 48 and st["batches"] < 48 and st["p99_us"] >= st["p50_us"] > 0
+    srv.close()
+
+
+def test_lru_eviction_under_tight_budget(M, O, pool):
+    sizes = [m["reordered"][1].size * 8 + m["perm"].size * 16 for m in pool]
+    srv = M.Server(hbm_budget_bytes=int(sum(sorted(sizes)[-2:]) * 1.3), window_us=100, lanes=2)
+    ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
+    outs = []
+    for rnd in range(3):
+        for j, m in enumerate(pool):
+            x = M.uniform(m["perm"].size, seed=rnd * 10 + j)
+            y = np.empty_like(x)
+            outs.append((j, x, y, srv.submit(ids[j], x, y)))
+    for j, x, y, t in outs:
+        assert srv.wait(t)[0] == M.MR_OK
+        rp, ci, v = pool[j]["orig"]
+        assert _rel(y, O.spmv_f64(rp, ci, v, x)) <= 1e-5
+    st = srv.stats()
+    assert st["evictions"] > 0 and st["admissions"] > len(pool)
+    srv.close()
+
+
+def test_refusal_and_timeout(M, pool):
+    srv = M.Server(hbm_budget_bytes=1 << 12, window_us=100)
+    mid = srv.add_matrix(*pool[0]["reordered"], pool[0]["perm"])
+    x = M.uniform(pool[0]["perm"].size, seed=1)
+    y = np.empty_like(x)
+    rc, _ = srv.wait(srv.submit(mid, x, y))
+    assert rc == M.MR_ERR_BUSY  # can never fit the budget
+    srv.close()
+    slow = M.Server(window_us=2_000_000)
+    mid = slow.add_matrix(*pool[3]["reordered"], pool[3]["perm"])
+    x = M.uniform(pool[3]["perm"].size, seed=2)
+    y = np.empty_like(x)
+    t = slow.submit(mid, x, y)
+    assert slow.wait(t, timeout_ms=10)[0] == M.MR_ERR_TIMEOUT
+    assert slow.wait(t, timeout_ms=10000)[0] == M.MR_OK
+    slow.close()
+    with pytest.raises(M.MRError):
+        M.Server().submit(99, x, y)
+
+
+def test_loadgen_poisson(M, pool):
+    srv = M.Server(window_us=200, lanes=3)
+    ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
+    xs = [M.uniform(m["perm"].size, seed=j) for j, m in enumerate(pool)]
+    ys = [np.empty_like(x) for x in xs]
+    srv.loadgen(ids, xs, ys, n_requests=2000, rate=5000.0, seed=3)
+    st = srv.stats()
+    assert st["completed"] == 2000 and st["req_per_s"] > 1000 and st["mean_batch"] >= 1
+    srv.close()

@@ -141,6 +141,36 @@ def test_persistent_and_two_kernel_forms_bit_identical(M, cases, sigma):
         p2.close()
 
 
+def test_hub_cache_bit_identical_and_reported(M):
+    """The shared-memory hub cache changes where x comes from, not the
+    arithmetic: results must equal the plan without it bit for bit. Skewed
+    R-MAT columns get a cache; a large banded matrix (no hot columns) not."""
+    import torch
+    rp, ci, v = M.gen_rmat(scale=18, edge_factor=16, seed=12)
+    n = rp.size - 1
+    A = M.view(_dev(rp), _dev(ci), _dev(v))
+    x = _dev(M.uniform(n, seed=3))
+    hub = M.MerbitPlan(A)
+    plain = M.MerbitPlan(A, hub_cache=False)
+    inf = hub.info()
+    assert inf.hub_columns > 0 and inf.hub_coverage >= 0.25
+    assert plain.info().hub_columns == 0
+    y1 = torch.empty_like(x)
+    y2 = torch.empty_like(x)
+    for _ in range(2):
+        hub.spmv(x, y1)
+        plain.spmv(x, y2)
+    torch.cuda.synchronize()
+    assert torch.equal(y1.view(torch.int32), y2.view(torch.int32))
+    # the descriptors are the reference format either way
+    assert all(np.array_equal(a, b) for a, b in zip(hub.descriptors(), plain.descriptors()))
+    hub.close()
+    plain.close()
+    rp, ci, v = M.gen_banded(1 << 20, 9, seed=1)
+    B = M.view(_dev(rp), _dev(ci), _dev(v))
+    assert M.MerbitPlan(B).info().hub_columns == 0
+
+
 def test_merbit_is_deterministic(M, cases):
     import torch
     rp, ci, v = cases["huge_row"]
