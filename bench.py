@@ -56,16 +56,23 @@ def spmv_bytes(n: int, nnz: int, val_bytes: int = 4) -> int:
     return 4 * (n + 1) + nnz * (4 + val_bytes) + 4 * n + 4 * n
 
 
-def traffic_from_profiles(name: str):
-    """DRAM bytes per launch recorded from an ncu capture (profiles/<name>)."""
+def traffic_from_profiles(name: str, bytes_step: int):
+    """DRAM bytes per launch from an ncu capture summarised in profiles/<name>
+    (lines `traffic_bytes_per_spmv:` and `algorithmic_bytes_per_spmv:`),
+    scaled to this workload by the ratio of algorithmic bytes (the capture
+    is a smaller matrix of the same family; traffic grows with it)."""
     p = os.path.join(REPO, "profiles", name)
+    got = {}
     try:
         for line in open(p):
-            if line.startswith("traffic_bytes_per_spmv:"):
-                return int(line.split(":")[1].split()[0])
+            for key in ("traffic_bytes_per_spmv", "algorithmic_bytes_per_spmv"):
+                if line.startswith(key + ":"):
+                    got[key] = int(line.split(":")[1].split()[0])
     except OSError:
-        pass
-    return None
+        return None, None
+    if len(got) < 2:
+        return None, None
+    return int(got["traffic_bytes_per_spmv"] * bytes_step / got["algorithmic_bytes_per_spmv"]), name
 
 
 class ClockSampler:
@@ -240,10 +247,12 @@ def run_ours(args):
         # threads per CTA and the hub cache on this matrix (setup, untimed)
         t0 = time.perf_counter()
         args.sigma, args.block, flags, _ = M.autotune(B, xp, yp, reps=5)
-        hub_cache = (flags & 1) == 0
         setup["autotune_s"] = round(time.perf_counter() - t0, 2)
+    else:
+        flags = 0
+    hub_cache = (flags & M.PLAN_NO_HUB_CACHE) == 0
     t0 = time.perf_counter()
-    plan = M.MerbitPlan(B, sigma=args.sigma, block=args.block, hub_cache=hub_cache)
+    plan = M.MerbitPlan(B, sigma=args.sigma, block=args.block, flags=flags)
     torch.cuda.synchronize()
     setup["plan_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
     bytes_step = spmv_bytes(n, nnz)
@@ -278,6 +287,24 @@ def run_ours(args):
         details["merbit_reordered_sigma14_block256_gbs"] = round(
             bytes_step / timed(lambda: plan_r.spmv(xp, yp), 50, 5) / 1e6, 1)
         plan_r.close()
+        # gather ceiling: x gathers alone over the same stream (no rows, no y)
+        g_ms = M.gather_ceiling(bci, bv, xp, reps=20)
+        details["gather_ceiling_gbs"] = round(bytes_step / g_ms / 1e6, 1)
+        # exact sector reuse-distance histograms (log2 bins, sector = 32
+        # columns) of the x-access stream before and after reordering, and
+        # the predictor's speedup estimate from the sampled histogram
+        log2_edges = [1 << k for k in range(21)]
+        for name, s_d in (("orig", ci_d), ("reordered", bci)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            counts, valid = M.rd_hist_exact(s_d, n, sector=32, edges=log2_edges)
+            rd_ms = (time.perf_counter() - t0) * 1e3
+            t0 = time.perf_counter()
+            sp, _ = M.locality_predict(s_d, n, graph_id=0)
+            lp_ms = (time.perf_counter() - t0) * 1e3
+            details[f"rd_{name}"] = {"log2_counts": counts.tolist(), "reuses": valid, "exact_ms": round(rd_ms, 1),
+                                     "predicted_speedup": round(sp, 4), "sampled_predict_ms": round(lp_ms, 2)}
+        details.update(laplace_companion(M, args, torch, timed, dev))
     inf = plan.info()
     details["hub_columns"] = inf.hub_columns
     details["hub_coverage"] = round(inf.hub_coverage, 4)
@@ -308,32 +335,19 @@ def run_ours(args):
     ms_step = ms_total / args.steps
     value = ws * bytes_step * args.steps / (ms_total / 1e3) / 1e9
 
-    # ---- e2e: host buffers through the C-ABI ----
+    # ---- e2e: host buffers through the C-ABI (mr_plain_requests: per step
+    # H2D of x from pinned memory, x' = P x, SpMV, y = P^T y', D2H of y,
+    # stream synchronise), timed on the host around the whole call ----
     k_e2e = max(1, min(args.steps, args.e2e_steps))
     x_h = torch.from_numpy(x).pin_memory()
     y_h = torch.empty(n, dtype=torch.float32).pin_memory()
-    x_in = torch.empty_like(x_d)
-    y_out = torch.empty_like(x_d)
-
-    def e2e_step():
-        x_in.copy_(x_h, non_blocking=True)
-        M.permute_vector(perm_d, x_in, xp, inverse=False)
-        plan.spmv(xp, yp)
-        M.permute_vector(perm_d, yp, y_out, inverse=True)
-        y_h.copy_(y_out, non_blocking=True)
-
-    for _ in range(3):
-        e2e_step()
+    xh_np, yh_np = x_h.numpy(), y_h.numpy()
+    M.plain_requests([plan], [B], [perm_d], np.zeros(3, np.int32), [xh_np] * 3, [yh_np] * 3)
     if dist:
         tdist.barrier()
     torch.cuda.synchronize()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(st)
-    for _ in range(k_e2e):
-        e2e_step()
-    f1.record(st)
-    torch.cuda.synchronize()
-    ms_e2e = f0.elapsed_time(f1)
+    ms_e2e, _ = M.plain_requests([plan], [B], [perm_d], np.zeros(k_e2e, np.int32), [xh_np] * k_e2e,
+                                 [yh_np] * k_e2e)
     if dist:
         t = torch.tensor([ms_e2e], device=dev)
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
@@ -344,16 +358,25 @@ def run_ours(args):
     y_csr = torch.empty_like(x_d)
     M.spmv_csr(A, x_d, y_csr)
     torch.cuda.synchronize()
-    got, ref = y_h.to(dev).double(), y_csr.double()
+    got, ref = y_h.to(dev).double(), y_csr.double()  # y_h: the last e2e result
     check = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
 
     peak, peak_kind = peaks()
     achieved = bytes_step / (ms_step / 1e3) / 1e9
-    traffic = traffic_from_profiles(f"merbit_spmv_rmat_s{args.scale}.md")
+    persistent = args.block == 1024
+    traffic, traffic_src = traffic_from_profiles(
+        f"merbit_persistent_hub_rmat_s21.md" if persistent and hub_cache else "merbit_persistent_kernel_rmat_s21.md",
+        bytes_step)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_spmv": bytes_step,
-                "kernels_timed": "one MERBIT SpMV (persistent kernel with fused fix-up, or grid kernel + fix-up)"}
+                "traffic_source": (f"profiles/{traffic_src}, R-MAT s21 capture scaled by algorithmic bytes"
+                                   if traffic_src else None),
+                "kernels_timed": ("merbit_persistent_kernel (one launch per SpMV, fused fix-up)" if persistent
+                                  else "merbit_spmv_kernel + merbit_fixup_kernel (two launches per SpMV)")}
+    if "gather_ceiling_gbs" in details:
+        roofline["gather_ceiling"] = {"achieved": details["gather_ceiling_gbs"], "unit": "GB/s",
+                                      "frac_of_ceiling": round(achieved / details["gather_ceiling_gbs"], 4)}
 
     cpu = None
     if rank == 0 and not args.quick and args.cpu_budget > 0:
@@ -377,16 +400,335 @@ def run_ours(args):
             "roofline": roofline,
             "e2e": {"value": round(e2e_val, 1), "unit": "GB/s", "h2d_bytes_per_step": 4 * n,
                     "d2h_bytes_per_step": 4 * n, "steps": k_e2e, "ms_per_step": round(ms_e2e / k_e2e, 4),
-                    "rel_l2_vs_fp64": check},
+                    "path": "mr_plain_requests (C-ABI, pinned host x/y, synchronised per step)",
+                    "rel_l2_vs_csr_orig": check},
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": (1 if persistent else 2) * args.steps,
             "details": {**details, **setup},
         }
         print(json.dumps(line), flush=True)
     if dist:
         tdist.barrier()
         tdist.destroy_process_group()
+    return 0
+
+
+def laplace_companion(M, args, torch, timed, dev):
+    """2D 5-point Laplacian on a 2048 x 2048 grid (4.19M rows, ~21M nnz,
+    FP32) with rows shuffled by a seeded permutation: plain CSR on the
+    shuffled matrix against MERBIT on its pGOrder reordering."""
+    d = lambda a: torch.from_numpy(a).to(dev)
+    rp, ci, v = M.gen_laplace2d(2048, shuffle=True, seed=args.seed)
+    n, nnz = rp.size - 1, ci.size
+    t0 = time.time()
+    n2o = M.pgorder(rp, ci, vsize=0, width=5)
+    t_ord = time.time() - t0
+    perm = np.empty(n, np.int32)
+    perm[n2o] = np.arange(n, dtype=np.int32)
+    rp_d, ci_d, v_d, perm_d = d(rp), d(ci), d(v), d(perm)
+    A = M.view(rp_d, ci_d, v_d)
+    brp, bci, bv = torch.empty_like(rp_d), torch.empty_like(ci_d), torch.empty_like(v_d)
+    M.permute_csr(A, perm_d, brp, bci, bv)
+    B = M.view(brp, bci, bv)
+    x = d(M.uniform(n, seed=args.seed + 1000))
+    y = torch.empty_like(x)
+    xp = torch.empty_like(x)
+    M.permute_vector(perm_d, x, xp, inverse=False)
+    b = spmv_bytes(n, nnz)
+    out = {"n_rows": n, "nnz": nnz, "pgorder_s": round(t_ord, 2)}
+    out["csr_shuffled_gbs"] = round(b / timed(lambda: M.spmv_csr(A, x, y), 50, 5) / 1e6, 1)
+    out["csr_reordered_gbs"] = round(b / timed(lambda: M.spmv_csr(B, xp, y), 50, 5) / 1e6, 1)
+    sg, bl, fl, _ = M.autotune(A, x, y, reps=3)
+    plan = M.MerbitPlan(A, sigma=sg, block=bl, flags=fl)
+    out["merbit_shuffled_gbs"] = round(b / timed(lambda: plan.spmv(x, y), 50, 5) / 1e6, 1)
+    plan.close()
+    sg, bl, fl, _ = M.autotune(B, xp, y, reps=3)
+    plan = M.MerbitPlan(B, sigma=sg, block=bl, flags=fl)
+    out["merbit_reordered_gbs"] = round(b / timed(lambda: plan.spmv(xp, y), 50, 5) / 1e6, 1)
+    out["merbit_reordered_sigma_block_flags"] = [sg, bl, fl]
+    plan.close()
+    return {"laplace2d_2048_shuffled": out}
+
+
+def run_serve(args):
+    """Serving workload: a resident pool of pGOrder-reordered FP16 matrices
+    (rows log-uniform 4K..2M, degree 4..64, R-MAT / banded / Chung-Lu),
+    Poisson requests, continuous batching; against the plain per-request FP32
+    path on the same matrix mix. Host x / y are page-locked on both paths."""
+    import torch
+    import mrb200 as M
+
+    rng = np.random.default_rng(args.seed)
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(a).to(dev)
+    cudart = torch.cuda.cudart()
+    protos = []
+    t0 = time.time()
+    for i in range(args.protos):
+        n = int(np.exp(rng.uniform(np.log(4096), np.log(2_000_000))))
+        deg = int(rng.integers(4, 65))
+        kind = i % 3
+        if kind == 0:
+            rp, ci, v = M.gen_rmat(n=n, edge_factor=deg, seed=args.seed + i)
+        elif kind == 1:
+            rp, ci, v = M.gen_banded(n, deg | 1, seed=args.seed + i)
+        else:
+            rp, ci, v = M.gen_chung_lu(n, 2.1, float(deg), 1, max(2, n // 10), seed=args.seed + i)
+        n2o = M.pgorder(rp, ci, vsize=0, width=5)
+        perm = np.empty(n, np.int32)
+        perm[n2o] = np.arange(n, dtype=np.int32)
+        A = M.view(d(rp), d(ci), d(v))
+        brp, bci, bv = torch.empty_like(A._keep[0]), torch.empty_like(A._keep[1]), torch.empty_like(A._keep[2])
+        M.permute_csr(A, d(perm), brp, bci, bv)
+        pr = dict(n=n, nnz=ci.size, kind=kind, orig=(rp, ci, v), perm=perm, brp=brp.cpu().numpy(),
+                  bci=bci.cpu().numpy(), bv16=bv.half().cpu().numpy(), bv32=bv.cpu().numpy(),
+                  x=M.uniform(n, seed=args.seed + 500 + i), y=np.empty(n, np.float32), ys=np.empty(n, np.float32))
+        # page-locked: admission uploads and request vectors move by DMA
+        for key in ("brp", "bci", "bv16", "perm", "x", "y", "ys"):
+            a = pr[key]
+            cudart.cudaHostRegister(a.ctypes.data, a.nbytes, 0)
+        protos.append(pr)
+    gen_s = time.time() - t0
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(free - 16 * 2**30)
+    srv = M.Server(hbm_budget_bytes=budget, window_us=args.window_us, max_batch=args.max_batch, lanes=args.lanes)
+    ids = []
+    t0 = time.time()
+    for r in range(args.pool):
+        p = protos[r % len(protos)]
+        ids.append(srv.add_matrix(p["brp"], p["bci"], p["bv16"], p["perm"]))
+    add_s = time.time() - t0
+    xs = [protos[r % len(protos)]["x"] for r in range(args.pool)]
+    ys = [protos[r % len(protos)]["ys"] for r in range(args.pool)]
+    # admit the whole pool once (uploads + plans), then measure
+    t0 = time.time()
+    srv.loadgen(ids, xs, ys, n_requests=args.pool, rate=1e6, seed=1)
+    warm_s = time.time() - t0
+    warm = srv.stats()
+    # accuracy of served FP16 results against an FP64 SpMV of the original
+    # (FP32-drawn) values, and against FP64 of the stored FP16 values
+    errs, errs_stored = [], []
+    for j, p in enumerate(protos):
+        y = np.empty(p["n"], np.float32)
+        rc, _ = srv.wait(srv.submit(ids[j], p["x"], y))
+        assert rc == M.MR_OK
+        rp, ci, v = p["orig"]
+        x64 = d(p["x"]).double().unsqueeze(1)
+        A64 = torch.sparse_csr_tensor(d(rp.astype(np.int64)), d(ci.astype(np.int64)), d(v).double(),
+                                      size=(p["n"], p["n"]))
+        ref = (A64 @ x64).squeeze(1)
+        errs.append(float(torch.linalg.norm(d(y).double() - ref) / torch.linalg.norm(ref)))
+        A16 = torch.sparse_csr_tensor(d(rp.astype(np.int64)), d(ci.astype(np.int64)),
+                                      d(v).half().double(), size=(p["n"], p["n"]))
+        ref16 = (A16 @ x64).squeeze(1)
+        errs_stored.append(float(torch.linalg.norm(d(y).double() - ref16) / torch.linalg.norm(ref16)))
+    srv.reset_stats()
+    sampler = ClockSampler(0)
+    sampler.start()
+    srv.loadgen(ids, xs, ys, n_requests=args.sat_requests, rate=1e7, seed=2)
+    sat = srv.stats()
+    srv.reset_stats()
+    srv.loadgen(ids, xs, ys, n_requests=int(args.rate * args.seconds), rate=args.rate, seed=3)
+    pois = srv.stats()
+    srv.close()
+    # plain per-request FP32 path over the same prototype mix
+    plans, views, perms = [], [], []
+    for p in protos:
+        B = M.view(d(p["brp"]), d(p["bci"]), d(p["bv32"]))
+        plans.append(M.MerbitPlan(B))
+        views.append(B)
+        perms.append(d(p["perm"]))
+    req = rng.integers(0, len(protos), args.plain_requests).astype(np.int32)
+    M.plain_requests(plans, views, perms, req[:20], [protos[k]["x"] for k in req[:20]],
+                     [protos[k]["y"] for k in req[:20]])
+    ms, lat = M.plain_requests(plans, views, perms, req, [protos[k]["x"] for k in req],
+                               [protos[k]["y"] for k in req])
+    clocks = sampler.stop()
+    plain_rps = args.plain_requests / (ms / 1e3)
+    mean_b16 = float(np.mean([spmv_bytes(p["n"], p["nnz"], 2) for p in protos]))
+    mean_b32 = float(np.mean([spmv_bytes(p["n"], p["nnz"], 4) for p in protos]))
+    line = {
+        "metric": "served_requests_per_s", "value": round(sat["req_per_s"], 1), "unit": "req/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f16 values, f32 x/accumulate", "data": "synthetic",
+        "config": {"workload": "serving pool", "pool": args.pool, "prototypes": args.protos,
+                   "rows": "log-uniform 4K-2M", "degree": "4-64", "kinds": "R-MAT / banded / Chung-Lu",
+                   "window_us": args.window_us, "max_batch": args.max_batch, "lanes": args.lanes,
+                   "host_vectors": "page-locked (both paths)", "hbm_budget_gb": round(budget / 2**30, 1)},
+        "saturation": {**{k: round(sat[k], 1) for k in ("req_per_s", "p50_us", "p99_us", "mean_batch")},
+                       "completed": sat["completed"],
+                       "gbs": round(sat["req_per_s"] * mean_b16 / 1e9, 1)},
+        "poisson": {"rate": args.rate, **{k: round(pois[k], 1) for k in ("req_per_s", "p50_us", "p99_us",
+                                                                          "mean_batch")},
+                    "completed": pois["completed"], "evictions": pois["evictions"]},
+        "plain_fp32_per_request": {"req_per_s": round(plain_rps, 1), "p50_us": round(float(np.median(lat)), 1),
+                                   "p99_us": round(float(np.percentile(lat, 99)), 1),
+                                   "gbs": round(plain_rps * mean_b32 / 1e9, 1)},
+        "speedup_vs_plain": round(sat["req_per_s"] / plain_rps, 2),
+        "max_rel_l2_vs_fp64": max(errs), "max_rel_l2_vs_fp64_of_stored_values": max(errs_stored),
+        "clocks": clocks,
+        "setup": {"gen_s": round(gen_s, 1), "add_pool_s": round(add_s, 2), "admit_pool_s": round(warm_s, 1),
+                  "admissions": warm["admissions"], "resident_gb": round(warm["resident_bytes"] / 2**30, 1),
+                  "mean_nnz": int(np.mean([p["nnz"] for p in protos])),
+                  "mean_rows": int(np.mean([p["n"] for p in protos]))},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_precision(args):
+    """Precision workload: Chung-Lu power law (8M rows, exponent 2.1, mean
+    degree 20, degrees clamped to [1, 200k]); values stored FP16 / BF16
+    (rounded from the drawn values), x FP32, FP32 accumulation with the FP64
+    carry fix-up; errors against an FP64 SpMV (torch sparse CSR, float64)."""
+    import torch
+    import mrb200 as M
+
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(a).to(dev)
+    t0 = time.time()
+    rp, ci, v = M.gen_chung_lu(args.cl_rows, 2.1, 20.0, 1, 200000, seed=args.seed)
+    gen_s = time.time() - t0
+    n, nnz = rp.size - 1, ci.size
+    x = M.uniform(n, seed=args.seed + 7)
+    rp_d, ci_d, v_d, x_d = d(rp), d(ci), d(v), d(x)
+    rp64, ci64 = rp_d.long(), ci_d.long()
+    x64 = x_d.double().unsqueeze(1)
+
+    def fp64(vals):
+        A = torch.sparse_csr_tensor(rp64, ci64, vals.double(), size=(n, n))
+        return (A @ x64).squeeze(1)
+
+    ref_orig = fp64(v_d)
+    absrow = (torch.sparse_csr_tensor(rp64, ci64, v_d.double().abs(), size=(n, n)) @ x64.abs()).squeeze(1)
+    absrow = torch.clamp(absrow, min=1e-30)
+    out = {}
+    for name, dt in (("f32", torch.float32), ("f16", torch.float16), ("bf16", torch.bfloat16)):
+        vals = v_d.to(dt)
+        A = M.view(rp_d, ci_d, vals)
+        y = torch.empty_like(x_d)
+        s_, b_, f_, _ = M.autotune(A, x_d, y, reps=3)
+        plan = M.MerbitPlan(A, sigma=s_, block=b_, flags=f_)
+        for _ in range(3):
+            plan.spmv(x_d, y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            plan.spmv(x_d, y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        yd = y.double()
+        ref_stored = fp64(vals)
+        out[name] = {
+            "rel_l2_vs_fp64_drawn": float(torch.linalg.norm(yd - ref_orig) / torch.linalg.norm(ref_orig)),
+            "rel_l2_vs_fp64_stored": float(torch.linalg.norm(yd - ref_stored) / torch.linalg.norm(ref_stored)),
+            "max_row_err_vs_fp64_drawn": float(((yd - ref_orig).abs() / absrow).max()),
+            "max_row_err_vs_fp64_stored": float(((yd - ref_stored).abs() / absrow).max()),
+            "ms": round(ms, 4), "gbs": round(spmv_bytes(n, nnz, vals.element_size()) / ms / 1e6, 1),
+            "sigma_block_flags": [s_, b_, f_],
+        }
+        plan.close()
+    line = {"metric": "precision", "unit": "relative L2 vs FP64", "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": "Chung-Lu power law", "n_rows": n, "nnz": nnz, "gamma": 2.1, "mean_degree": 20,
+                       "max_degree": 200000, "order": "as generated"},
+            "results": out, "setup": {"gen_s": round(gen_s, 1),
+                                      "max_row_len": int(np.diff(rp).max())}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args):
+    """Batching workload: args.batch_count independent CSR matrices, rows
+    log-uniform in [1K, 512K], each R-MAT (edge factor 8-32) or banded
+    (bandwidth 3-65) by seeded choice, FP32 values / x uniform[-1,1], each
+    pGOrder-reordered on the GPU; sigma picked per size bucket by the
+    project's tuner; all SpMVs in one CUDA-graph launch of the batched
+    persistent kernels, against one mr_spmv_merbit launch per matrix with
+    the tuner's full choice."""
+    import torch
+    import mrb200 as M
+
+    rng = np.random.default_rng(args.seed)
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(a).to(dev)
+    t0 = time.time()
+    mats = []
+    for i in range(args.batch_count):
+        n = int(np.exp(rng.uniform(np.log(1024), np.log(512 * 1024))))
+        if rng.integers(0, 2) == 0:
+            rp, ci, v = M.gen_rmat(n=n, edge_factor=int(rng.integers(8, 33)), seed=args.seed + i)
+        else:
+            rp, ci, v = M.gen_banded(n, int(rng.integers(1, 33)) * 2 + 1, seed=args.seed + i)
+        n2o = M.pgorder(rp, ci, vsize=0, width=5)
+        perm = np.empty(n, np.int32)
+        perm[n2o] = np.arange(n, dtype=np.int32)
+        A = M.view(d(rp), d(ci), d(v))
+        brp, bci, bv = torch.empty_like(A._keep[0]), torch.empty_like(A._keep[1]), torch.empty_like(A._keep[2])
+        M.permute_csr(A, d(perm), brp, bci, bv)
+        mats.append((M.view(brp, bci, bv), n, ci.size))
+        del A
+    gen_s = time.time() - t0
+    total_bytes = sum(spmv_bytes(n, nnz) for _, n, nnz in mats)
+    xs = [d(M.uniform(n, seed=7 + i)) for i, (_, n, _) in enumerate(mats)]
+    ys = [torch.empty_like(x) for x in xs]
+    tuner = M.Tuner()
+    t0 = time.time()
+    picks = [tuner.pick(B, x, y) for (B, _, _), x, y in zip(mats, xs, ys)]
+    tune_s = time.time() - t0
+    buckets, tuned = tuner.stats()
+    plans = [M.MerbitPlan(B, sigma=s_, block=b_, flags=f_) for (B, _, _), (s_, b_, f_) in zip(mats, picks)]
+    st = torch.cuda.Stream()
+    batch = M.Batch([(p, x, y) for p, x, y in zip(plans, xs, ys)], stream=st)
+    groups, tiles = batch.info()
+    batch.capture(st)
+
+    def time_it(fn, steps):
+        for _ in range(3):
+            fn()
+        st.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_graph = time_it(lambda: batch.launch(st), args.steps)
+
+    def per_matrix():
+        for p, x, y in zip(plans, xs, ys):
+            p.spmv(x, y, stream=st)
+
+    ms_loop = time_it(per_matrix, max(3, args.steps // 10))
+    # results: graph replay is bitwise the same as the per-matrix launches
+    want = [y.clone() for y in ys]
+    batch.launch(st)
+    st.synchronize()
+    identical = all(torch.equal(a.view(torch.int32), b.view(torch.int32)) for a, b in zip(ys, want))
+    peak, peak_kind = peaks()
+    gbs = total_bytes / ms_graph / 1e6
+    line = {"metric": "batched_spmv_hbm_gbs", "value": round(gbs, 1), "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "ms_per_step": round(ms_graph, 4), "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "batched independent matrices, one CUDA-graph launch", "count": len(mats),
+                       "rows": "log-uniform 1K-512K", "kinds": "R-MAT ef 8-32 / banded bw 3-65",
+                       "total_rows": int(sum(n for _, n, _ in mats)), "total_nnz": int(sum(z for _, _, z in mats)),
+                       "groups": groups, "tiles": tiles},
+            "per_matrix_launches": {"ms_per_step": round(ms_loop, 4), "gbs": round(total_bytes / ms_loop / 1e6, 1),
+                                    "launches": len(mats)},
+            "graph_speedup_vs_per_matrix": round(ms_loop / ms_graph, 2),
+            "graph_identical_to_per_matrix": bool(identical),
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "peak_kind": peak_kind},
+            "tuner": {"buckets": buckets, "tuned": tuned, "tune_s": round(tune_s, 1),
+                      "sigmas": sorted(set(p[0] for p in picks))},
+            "setup": {"gen_reorder_s": round(gen_s, 1)}}
+    batch.close()
+    tuner.close()
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -405,11 +747,29 @@ def main() -> int:
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of CPU-baseline timing")
     ap.add_argument("--quick", action="store_true", help="skip companion numbers and CPU baseline")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="use --sigma/--block instead of the autotuner")
+    ap.add_argument("--workload", choices=["spmv", "serve", "precision", "batch"], default="spmv")
+    ap.add_argument("--cl-rows", type=int, default=8 * 1024 * 1024, help="precision: Chung-Lu rows")
+    ap.add_argument("--pool", type=int, default=2000, help="serve: resident matrices")
+    ap.add_argument("--protos", type=int, default=24, help="serve: distinct generated matrices in the pool")
+    ap.add_argument("--rate", type=float, default=20000.0, help="serve: Poisson arrivals per second")
+    ap.add_argument("--seconds", type=float, default=2.0, help="serve: length of the Poisson run")
+    ap.add_argument("--window-us", type=int, default=200)
+    ap.add_argument("--max-batch", type=int, default=64)
+    ap.add_argument("--lanes", type=int, default=3)
+    ap.add_argument("--sat-requests", type=int, default=20000)
+    ap.add_argument("--plain-requests", type=int, default=2000)
+    ap.add_argument("--batch-count", type=int, default=512, help="batch: matrices in the graph launch")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serve":
+        return run_serve(args)
+    if args.workload == "precision":
+        return run_precision(args)
+    if args.workload == "batch":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -215,7 +215,7 @@ typedef struct mr_server mr_server;
 typedef struct mr_server_config {
     int64_t hbm_budget_bytes; /* device bytes for resident matrices; 0 = half the free memory */
     int32_t window_us;        /* batching window (default 200) */
-    int32_t max_batch;        /* requests per batch (default 256) */
+    int32_t max_batch;        /* requests per batch (default 64) */
     int32_t lanes;            /* batches in flight, one stream each (default 3) */
     int32_t sigma;            /* MERBIT sigma of resident plans (default 14) */
 } mr_server_config;
@@ -232,7 +232,10 @@ int mr_server_add_matrix(mr_server* server, int32_t n, int64_t nnz, const int32_
                          const int32_t* colidx_host, const void* vals_host, int32_t dtype,
                          const int32_t* perm_old2new_host, int32_t* id);
 /* Queues y = A_id x; x_host must stay valid and y_host writable until the
- * request completes (mr_server_wait / mr_server_drain). */
+ * request completes (mr_server_wait / mr_server_drain). Vectors in
+ * page-locked host memory (cudaHostAlloc, or cudaHostRegister covering the
+ * whole vector) are copied by DMA straight from / into the caller's buffer;
+ * other host memory is staged through the server's pinned buffers. */
 int mr_server_submit(mr_server* server, int32_t id, const float* x_host, float* y_host, uint64_t* ticket);
 /* Waits up to timeout_ms (MR_ERR_TIMEOUT after); returns the request's status. */
 int mr_server_wait(mr_server* server, uint64_t ticket, int32_t timeout_ms, double* latency_us);
@@ -244,6 +247,26 @@ int mr_server_destroy(mr_server* server);
  * over the ids (uniform), x_of[k] / y_of[k] host buffers of ids[k]. */
 int mr_server_loadgen(mr_server* server, const int32_t* ids, int32_t n_ids, int64_t n_requests, double rate,
                       uint64_t seed, const float* const* x_of, float* const* y_of, int32_t timeout_ms);
+
+/* The plain per-request path the server is compared with: request r runs
+ * alone on `stream` (H2D x, x' = P x, MERBIT SpMV with plans[req_mat[r]],
+ * y = P^T y', D2H, synchronise). views/plans/perm_dev per matrix; x_host /
+ * y_host per request, page-locked ones copied directly as in
+ * mr_server_submit; elapsed_ms and lat_us (per request) may be NULL. */
+int mr_plain_requests(int32_t n_mats, const mr_merbit_plan* const* plans, const mr_csr_view* views,
+                      const int32_t* const* perm_dev, int64_t n_requests, const int32_t* req_mat,
+                      const float* const* x_host, float* const* y_host, void* stream, double* elapsed_ms,
+                      double* lat_us);
+
+/* Gather ceiling of a column-index stream: time per pass (ms, mean of reps
+ * after two warm-up passes) of a kernel that streams colidx / vals with
+ * 16-byte evict-first loads and gathers x[colidx[k]] once per nonzero, with
+ * no row structure and no y. A lower bound for any SpMV that gathers x once
+ * per nonzero on the same stream; no reference counterpart (measurement
+ * only). colidx and vals 16-byte aligned; the last nnz % 4 entries are left
+ * out. */
+int mr_gather_ceiling(const int32_t* colidx_dev, const float* vals_dev, int64_t nnz, const float* x_dev,
+                      int32_t reps, float* ms_per_pass, void* stream);
 
 /* ------------------------------------------------------ permutation ---- */
 

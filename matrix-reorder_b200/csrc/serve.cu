@@ -1,8 +1,7 @@
 // Serving loop: device-resident pool of (reordered) matrices, continuous
 // batching of SpMV requests, p50/p99 latency.
 //
-// No counterpart in the reference (a one-matrix-per-process harness); this is
-// the serving form BASELINE.json's north_star asks for.
+// No counterpart in the reference (a one-matrix-per-process harness).
 //
 //  * Pool: matrices are registered with host CSR arrays (borrowed: the caller
 //    keeps them alive) and an optional permutation perm[old] = new; requests
@@ -15,11 +14,18 @@
 //    arrival order, admits their matrices and launches the batch on a free
 //    lane (stream); up to `lanes` batches are in flight, so requests that
 //    arrive while others are on the GPU form the next batch and overlap on
-//    the device (continuous batching). A batch is: one H2D copy of all x,
-//    one batched permutation, the batched MERBIT kernels (one per (sigma,
-//    dtype) group), one batched un-permutation, one D2H copy.
+//    the device (continuous batching). A batch is: the H2D copies of its x
+//    vectors, one batched permutation, the batched MERBIT kernels (one per
+//    (sigma, dtype) group), one batched un-permutation, the D2H copies. The
+//    scheduler issues a batch without holding the server lock, so submits
+//    are never blocked behind the launch.
+//  * Host vectors: x and y in page-locked memory (cudaHostAlloc, or
+//    cudaHostRegister over the whole vector) are copied by the copy engines
+//    straight from / into the caller's buffer; other host memory goes
+//    through the lane's pinned staging area with a host memcpy.
 //  * Completion: a thread waits on each lane's event in launch order, copies
-//    results to the callers' y, records latency (submit -> result in y).
+//    staged results to the callers' y, records latency (submit -> result in
+//    y).
 //  * Determinism: every request's SpMV runs the same tiles with the same
 //    order of operations whatever else is in its batch, so its result is
 //    bitwise the same alone and in the mix.
@@ -30,10 +36,13 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <random>
+#include <set>
 #include <thread>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -86,11 +95,23 @@ __global__ void batch_permute_kernel(const PermOp* __restrict__ ops, const long 
     }
 }
 
+// page-locked host memory (allocated or registered with the CUDA runtime)
+bool host_pinned(const void* p)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 struct Request {
     uint64_t ticket = 0;
     int id = 0;
     const float* x = nullptr;
     float* y = nullptr;
+    bool x_pinned = false, y_pinned = false;  // page-locked: copied without staging
     Clock::time_point t_submit;
     double latency_us = 0.0;
     int status = MR_OK;
@@ -168,6 +189,7 @@ struct Lane {
     std::vector<Request*> reqs;
     std::vector<long long> off;
     std::vector<int> mats;
+    std::vector<Matrix*> mp;  // the batch's matrices, read by launch_batch without the lock
     bool busy = false;
 };
 
@@ -177,7 +199,7 @@ struct mr_server {
     mr_server_config cfg{};
     std::mutex mu;
     std::condition_variable cv_sched, cv_done, cv_lane;
-    std::vector<Matrix> mats;
+    std::vector<std::unique_ptr<Matrix>> mats;  // stable addresses: batches read them unlocked
     std::deque<Request*> pending;
     std::unordered_map<uint64_t, Request*> reqs;
     std::vector<Lane> lanes;
@@ -194,6 +216,7 @@ struct mr_server {
     int64_t submitted = 0, completed = 0, batches = 0, admissions = 0, evictions = 0, rejected = 0, batch_items = 0;
     Clock::time_point t_first{}, t_last{};
     bool have_first = false;
+    std::set<std::tuple<const void*, const void*, const void*, int32_t, int64_t>> validated;
 };
 
 namespace {
@@ -272,13 +295,13 @@ bool make_room(mr_server* s, size_t need, const std::vector<int>& keep)
     while (s->resident_bytes + need > (size_t)s->cfg.hbm_budget_bytes) {
         int victim = -1;
         for (int i = 0; i < (int)s->mats.size(); ++i) {
-            const Matrix& m = s->mats[(size_t)i];
+            const Matrix& m = *s->mats[(size_t)i];
             if (!m.resident || m.refs > 0) continue;
             if (std::find(keep.begin(), keep.end(), i) != keep.end()) continue;
-            if (victim < 0 || m.last_use < s->mats[(size_t)victim].last_use) victim = i;
+            if (victim < 0 || m.last_use < s->mats[(size_t)victim]->last_use) victim = i;
         }
         if (victim < 0) return false;
-        Matrix& v = s->mats[(size_t)victim];
+        Matrix& v = *s->mats[(size_t)victim];
         free_resident(v, s->admit_st);
         s->resident_bytes -= v.bytes;
         ++s->evictions;
@@ -290,12 +313,18 @@ int launch_batch(mr_server* s, Lane& L)
 {
     const int count = (int)L.reqs.size();
     L.off.assign((size_t)count + 1, 0);
-    for (int i = 0; i < count; ++i) L.off[(size_t)i + 1] = L.off[(size_t)i] + s->mats[(size_t)L.mats[(size_t)i]].n;
+    for (int i = 0; i < count; ++i) L.off[(size_t)i + 1] = L.off[(size_t)i] + L.mp[(size_t)i]->n;
     const long long total = L.off[(size_t)count];
-    MR_TRY(L.hx.reserve((size_t)total + 1));
-    MR_TRY(L.hy.reserve((size_t)total + 1));
+    bool staged = false;
+    for (const Request* r : L.reqs) staged = staged || !r->x_pinned || !r->y_pinned;
+    if (staged) {
+        MR_TRY(L.hx.reserve((size_t)total + 1));
+        MR_TRY(L.hy.reserve((size_t)total + 1));
+    }
     for (int i = 0; i < count; ++i)
-        std::memcpy(L.hx.p + L.off[(size_t)i], L.reqs[(size_t)i]->x, sizeof(float) * (size_t)(L.off[(size_t)i + 1] - L.off[(size_t)i]));
+        if (!L.reqs[(size_t)i]->x_pinned)
+            std::memcpy(L.hx.p + L.off[(size_t)i], L.reqs[(size_t)i]->x,
+                        sizeof(float) * (size_t)(L.off[(size_t)i + 1] - L.off[(size_t)i]));
     const size_t vbytes = sizeof(float) * (size_t)(total + 1);
     MR_TRY(L.dx.reserve(vbytes, L.st));
     MR_TRY(L.dxp.reserve(vbytes, L.st));
@@ -306,7 +335,7 @@ int launch_batch(mr_server* s, Lane& L)
     long long carry_total = 0;
     std::vector<long long> carry_off((size_t)count);
     for (int i = 0; i < count; ++i) {
-        const Matrix& m = s->mats[(size_t)L.mats[(size_t)i]];
+        const Matrix& m = *L.mp[(size_t)i];
         groups[{m.plan.sigma, m.dtype}].push_back(i);
         carry_off[(size_t)i] = carry_total;
         carry_total += std::max(m.plan.tile_num, 1);
@@ -340,7 +369,7 @@ int launch_batch(mr_server* s, Lane& L)
         GroupLaunch x{dtype, sigma, (int)g.second.size(), at, prefix_host.size(), 0};
         prefix_host.push_back(0);
         for (int i : g.second) {
-            const Matrix& m = s->mats[(size_t)L.mats[(size_t)i]];
+            const Matrix& m = *L.mp[(size_t)i];
             const mr_csr_view A{m.n, m.n, m.nnz, m.d_rowptr, m.d_colidx, m.d_vals, m.dtype};
             MR_TRY(batch_fill_op(ops_host.data() + at, dtype, sigma, m.plan, A, dxp + L.off[(size_t)i],
                                  dyp + L.off[(size_t)i], carry + carry_off[(size_t)i]));
@@ -352,11 +381,15 @@ int launch_batch(mr_server* s, Lane& L)
         gl.push_back(x);
     }
     for (int i = 0; i < count; ++i) {
-        const Matrix& m = s->mats[(size_t)L.mats[(size_t)i]];
+        const Matrix& m = *L.mp[(size_t)i];
         pops[(size_t)i] = PermOp{m.d_perm, L.off[(size_t)i], m.n};
     }
     cudaStream_t st = L.st;
-    MR_CUDA_TRY(cudaMemcpyAsync(dx, L.hx.p, sizeof(float) * (size_t)total, cudaMemcpyHostToDevice, st));
+    for (int i = 0; i < count; ++i) {
+        const Request* r = L.reqs[(size_t)i];
+        const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
+        MR_CUDA_TRY(cudaMemcpyAsync(dx + o, r->x_pinned ? r->x : L.hx.p + o, nb, cudaMemcpyHostToDevice, st));
+    }
     // the small tables go through pageable memory; the copy is synchronous
     // with respect to the host buffer, which is then free to reuse
     MR_CUDA_TRY(cudaMemcpyAsync(L.ops.p, ops_host.data(), at, cudaMemcpyHostToDevice, st));
@@ -375,7 +408,11 @@ int launch_batch(mr_server* s, Lane& L)
                                 static_cast<const long long*>(L.prefix.p) + g.prefix_at, g.count, g.tiles, st));
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
     MR_CUDA_TRY(cudaGetLastError());
-    MR_CUDA_TRY(cudaMemcpyAsync(L.hy.p, dy, sizeof(float) * (size_t)total, cudaMemcpyDeviceToHost, st));
+    for (int i = 0; i < count; ++i) {
+        const Request* r = L.reqs[(size_t)i];
+        const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
+        MR_CUDA_TRY(cudaMemcpyAsync(r->y_pinned ? r->y : L.hy.p + o, dy + o, nb, cudaMemcpyDeviceToHost, st));
+    }
     MR_CUDA_TRY(cudaEventRecord(L.done, st));
     return MR_OK;
 }
@@ -422,12 +459,13 @@ void scheduler_loop(mr_server* s)
         Lane& L = s->lanes[(size_t)lane];
         L.reqs.clear();
         L.mats.clear();
+        L.mp.clear();
         std::vector<int> keep;
         std::deque<Request*> deferred;
         while (!s->pending.empty() && (int)L.reqs.size() < s->cfg.max_batch) {
             Request* r = s->pending.front();
             s->pending.pop_front();
-            Matrix& m = s->mats[(size_t)r->id];
+            Matrix& m = *s->mats[(size_t)r->id];
             if (!m.resident) {
                 const size_t need = matrix_bytes(m);
                 if (need > (size_t)s->cfg.hbm_budget_bytes) {  // can never fit
@@ -453,6 +491,7 @@ void scheduler_loop(mr_server* s)
             keep.push_back(r->id);
             L.reqs.push_back(r);
             L.mats.push_back(r->id);
+            L.mp.push_back(&m);
         }
         for (auto it = deferred.rbegin(); it != deferred.rend(); ++it) s->pending.push_front(*it);
         if (L.reqs.empty()) {
@@ -461,9 +500,11 @@ void scheduler_loop(mr_server* s)
             continue;
         }
         L.busy = true;
+        lk.unlock();
         const int rc = launch_batch(s, L);
+        lk.lock();
         if (rc != MR_OK) {
-            for (int id : L.mats) --s->mats[(size_t)id].refs;
+            for (int id : L.mats) --s->mats[(size_t)id]->refs;
             finish_requests(s, L.reqs, rc);
             L.busy = false;
             s->cv_done.notify_all();
@@ -490,10 +531,11 @@ void completion_loop(mr_server* s)
         // results to the callers' buffers
         if (e == cudaSuccess)
             for (size_t i = 0; i < L.reqs.size(); ++i)
-                std::memcpy(L.reqs[i]->y, L.hy.p + L.off[i], sizeof(float) * (size_t)(L.off[i + 1] - L.off[i]));
+                if (!L.reqs[i]->y_pinned)
+                    std::memcpy(L.reqs[i]->y, L.hy.p + L.off[i], sizeof(float) * (size_t)(L.off[i + 1] - L.off[i]));
         lk.lock();
         s->inflight.pop_front();
-        for (int id : L.mats) --s->mats[(size_t)id].refs;
+        for (int id : L.mats) --s->mats[(size_t)id]->refs;
         finish_requests(s, L.reqs, e == cudaSuccess ? MR_OK : MR_ERR_CUDA);
         L.reqs.clear();
         L.busy = false;
@@ -515,7 +557,7 @@ int mr_server_create(const mr_server_config* cfg, mr_server** out)
     if (!s) return MR_ERR_NOMEM;
     if (cfg) s->cfg = *cfg;
     if (s->cfg.window_us <= 0) s->cfg.window_us = 200;
-    if (s->cfg.max_batch <= 0) s->cfg.max_batch = 256;
+    if (s->cfg.max_batch <= 0) s->cfg.max_batch = 64;
     if (s->cfg.lanes <= 0) s->cfg.lanes = 3;
     if (s->cfg.sigma <= 0) s->cfg.sigma = 14;
     if (!merbit_sigma_supported(s->cfg.sigma) || s->cfg.lanes > 16) {
@@ -550,21 +592,32 @@ int mr_server_add_matrix(mr_server* s, int32_t n, int64_t nnz, const int32_t* ro
     if (!s || !id || n <= 0 || nnz < 0 || nnz > INT32_MAX || !rowptr || (nnz > 0 && (!colidx || !vals)))
         return MR_ERR_INVALID_ARG;
     if (dtype != MR_F32 && dtype != MR_F16 && dtype != MR_BF16) return MR_ERR_UNSUPPORTED;
-    // host-side validation (the pool admits matrices without a device check)
-    if (rowptr[0] != 0 || rowptr[n] != nnz) return MR_ERR_INVALID_ARG;
-    for (int32_t i = 0; i < n; ++i)
-        if (rowptr[i + 1] < rowptr[i]) return MR_ERR_INVALID_ARG;
-    for (int64_t k = 0; k < nnz; ++k)
-        if (colidx[k] < 0 || colidx[k] >= n) return MR_ERR_INVALID_ARG;
-    if (perm_old2new) {
-        std::vector<char> seen((size_t)n, 0);
-        for (int32_t i = 0; i < n; ++i) {
-            const int32_t p = perm_old2new[i];
-            if (p < 0 || p >= n || seen[(size_t)p]) return MR_ERR_INVALID_PERM;
-            seen[(size_t)p] = 1;
+    // host-side validation (the pool admits matrices without a device
+    // check); arrays already validated for an earlier registration are not
+    // scanned again (the caller keeps registered arrays unchanged)
+    const auto key = std::make_tuple((const void*)rowptr, (const void*)colidx, (const void*)perm_old2new, n, nnz);
+    bool known;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        known = s->validated.count(key) > 0;
+    }
+    if (!known) {
+        if (rowptr[0] != 0 || rowptr[n] != nnz) return MR_ERR_INVALID_ARG;
+        for (int32_t i = 0; i < n; ++i)
+            if (rowptr[i + 1] < rowptr[i]) return MR_ERR_INVALID_ARG;
+        for (int64_t k = 0; k < nnz; ++k)
+            if (colidx[k] < 0 || colidx[k] >= n) return MR_ERR_INVALID_ARG;
+        if (perm_old2new) {
+            std::vector<char> seen((size_t)n, 0);
+            for (int32_t i = 0; i < n; ++i) {
+                const int32_t p = perm_old2new[i];
+                if (p < 0 || p >= n || seen[(size_t)p]) return MR_ERR_INVALID_PERM;
+                seen[(size_t)p] = 1;
+            }
         }
     }
     std::lock_guard<std::mutex> lk(s->mu);
+    s->validated.insert(key);
     Matrix m;
     m.n = n;
     m.nnz = nnz;
@@ -573,7 +626,9 @@ int mr_server_add_matrix(mr_server* s, int32_t n, int64_t nnz, const int32_t* ro
     m.h_colidx = colidx;
     m.h_vals = vals;
     m.h_perm = perm_old2new;
-    s->mats.push_back(m);
+    auto pm = std::unique_ptr<Matrix>(new (std::nothrow) Matrix(m));
+    if (!pm) return MR_ERR_NOMEM;
+    s->mats.push_back(std::move(pm));
     *id = (int32_t)s->mats.size() - 1;
     return MR_OK;
 }
@@ -586,6 +641,8 @@ int mr_server_submit(mr_server* s, int32_t id, const float* x, float* y, uint64_
     r->id = id;
     r->x = x;
     r->y = y;
+    r->x_pinned = host_pinned(x);
+    r->y_pinned = host_pinned(y);
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -656,7 +713,7 @@ int mr_server_get_stats(mr_server* s, mr_server_stats* out)
     st.evictions = s->evictions;
     st.resident_bytes = (int64_t)s->resident_bytes;
     int64_t nres = 0;
-    for (const auto& m : s->mats) nres += m.resident ? 1 : 0;
+    for (const auto& m : s->mats) nres += m->resident ? 1 : 0;
     st.resident_matrices = nres;
     st.mean_batch = s->batches ? (double)s->batch_items / (double)s->batches : 0.0;
     if (!s->lat.empty()) {
@@ -708,7 +765,7 @@ int mr_server_destroy(mr_server* s)
     if (s->compl_.joinable()) s->compl_.join();
     cudaDeviceSynchronize();
     for (auto& m : s->mats)
-        if (m.resident) free_resident(m, s->admit_st);
+        if (m->resident) free_resident(*m, s->admit_st);
     for (auto& L : s->lanes) {
         for (DevVec* d : {&L.dx, &L.dxp, &L.dyp, &L.dy, &L.carry, &L.ops, &L.prefix, &L.pops, &L.pprefix})
             if (d->p) cudaFreeAsync(d->p, s->admit_st);
@@ -746,6 +803,56 @@ int mr_server_loadgen(mr_server* s, const int32_t* ids, int32_t n_ids, int64_t n
         MR_TRY(mr_server_submit(s, ids[k], x_of[k], y_of[k], nullptr));
     }
     return mr_server_drain(s, timeout_ms);
+}
+
+// Plain per-request path (the comparison baseline for the server): each
+// request in turn copies x to the device, permutes it, runs one MERBIT SpMV
+// with its own plan, un-permutes y, copies it back and synchronises. Host
+// vectors follow the server's rule: page-locked ones are copied directly,
+// others through a pinned staging buffer.
+int mr_plain_requests(int32_t n_mats, const mr_merbit_plan* const* plans, const mr_csr_view* views,
+                      const int32_t* const* perm_dev, int64_t n_requests, const int32_t* req_mat,
+                      const float* const* x_host, float* const* y_host, void* stream, double* elapsed_ms,
+                      double* lat_us)
+{
+    if (n_mats <= 0 || !plans || !views || !perm_dev || n_requests < 0 || !req_mat || !x_host || !y_host)
+        return MR_ERR_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    int32_t nmax = 0;
+    for (int i = 0; i < n_mats; ++i) {
+        if (!plans[i] || views[i].n_rows != views[i].n_cols) return MR_ERR_INVALID_ARG;
+        nmax = std::max(nmax, views[i].n_rows);
+    }
+    for (int64_t r = 0; r < n_requests; ++r)
+        if (req_mat[r] < 0 || req_mat[r] >= n_mats || !x_host[r] || !y_host[r]) return MR_ERR_INVALID_ARG;
+    PinnedVec<float> hx, hy;
+    MR_TRY(hx.reserve((size_t)nmax + 1));
+    MR_TRY(hy.reserve((size_t)nmax + 1));
+    DevBuf dx, dxp, dyp, dy;
+    MR_TRY(dx.alloc(sizeof(float) * ((size_t)nmax + 1), st));
+    MR_TRY(dxp.alloc(sizeof(float) * ((size_t)nmax + 1), st));
+    MR_TRY(dyp.alloc(sizeof(float) * ((size_t)nmax + 1), st));
+    MR_TRY(dy.alloc(sizeof(float) * ((size_t)nmax + 1), st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));
+    const auto t0 = Clock::now();
+    for (int64_t r = 0; r < n_requests; ++r) {
+        const auto tr = Clock::now();
+        const int k = req_mat[r];
+        const int n = views[k].n_rows;
+        const size_t nb = sizeof(float) * (size_t)n;
+        const bool xp = host_pinned(x_host[r]), yp = host_pinned(y_host[r]);
+        if (!xp) std::memcpy(hx.p, x_host[r], nb);
+        MR_CUDA_TRY(cudaMemcpyAsync(dx.p, xp ? x_host[r] : hx.p, nb, cudaMemcpyHostToDevice, st));
+        MR_TRY(launch_permute_vector(n, perm_dev[k], dx.as<float>(), dxp.as<float>(), 0, st));
+        MR_TRY(mr_spmv_merbit(plans[k], &views[k], dxp.as<float>(), dyp.as<float>(), stream));
+        MR_TRY(launch_permute_vector(n, perm_dev[k], dyp.as<float>(), dy.as<float>(), 1, st));
+        MR_CUDA_TRY(cudaMemcpyAsync(yp ? y_host[r] : hy.p, dy.p, nb, cudaMemcpyDeviceToHost, st));
+        MR_CUDA_TRY(cudaStreamSynchronize(st));
+        if (!yp) std::memcpy(y_host[r], hy.p, nb);
+        if (lat_us) lat_us[r] = std::chrono::duration<double, std::micro>(Clock::now() - tr).count();
+    }
+    if (elapsed_ms) *elapsed_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    return MR_OK;
 }
 
 }  // extern "C"

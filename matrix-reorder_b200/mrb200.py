@@ -31,6 +31,12 @@ MR_ERR_PREDICT = 10
 
 MR_F32, MR_F16, MR_BF16 = 0, 1, 2
 MODEL_MERBIT_SAMPLED, MODEL_MERBIT_EXACT, MODEL_CSR_SAMPLED, MODEL_CSR_EXACT = 0, 1, 2, 3
+# plan flags (include/mr.h MR_PLAN_*)
+PLAN_NO_HUB_CACHE, PLAN_GATHER_NO_L1, PLAN_GATHER_L2_ONLY, PLAN_SMALL_HUB_CACHE = 1, 2, 4, 8
+
+
+def PLAN_HUB_LIMIT(kcols: int) -> int:
+    return int(kcols) << 8
 
 # reference RD bins (src/class.cu:1267)
 REF_EDGES = [1, 112, 512, 18432, 36864, 73728, 147456, 294912, 589824]
@@ -153,10 +159,14 @@ def spmv_csr(A: CsrView, x, y, stream=None) -> None:
 class MerbitPlan:
     """Owner of an mr_merbit_plan (the reference's TILE<BLOCK,SIGMA>)."""
 
-    def __init__(self, A: CsrView, sigma: int = 14, block: int = 0, stream=None, hub_cache: bool = True):
+    def __init__(self, A: CsrView, sigma: int = 14, block: int = 0, stream=None, hub_cache: bool = True,
+                 flags: Optional[int] = None):
+        """flags: MR_PLAN_* bits (as returned by autotune); default from hub_cache."""
         h = C.c_void_p()
-        check(lib().mr_merbit_plan_create_ex(C.byref(A), sigma, block, 0 if hub_cache else 1, _stream(stream),
-                                             C.byref(h)), "mr_merbit_plan_create_ex")
+        if flags is None:
+            flags = 0 if hub_cache else PLAN_NO_HUB_CACHE
+        check(lib().mr_merbit_plan_create_ex(C.byref(A), sigma, block, flags, _stream(stream), C.byref(h)),
+              "mr_merbit_plan_create_ex")
         self.h = h
         self.A = A
 
@@ -583,6 +593,7 @@ def _server_sigs(L):
     _sig(L.mr_server_reset_stats, C.c_int, vp)
     _sig(L.mr_server_destroy, C.c_int, vp)
     _sig(L.mr_server_loadgen, C.c_int, vp, vp, i32, i64, C.c_double, u64, vp, vp, i32)
+    _sig(L.mr_plain_requests, C.c_int, i32, vp, vp, vp, i64, vp, vp, vp, vp, P(C.c_double), vp)
     L._server_sigs = True
 
 
@@ -591,7 +602,7 @@ class Server:
     Host arrays passed to add_matrix / submit are kept referenced here for
     as long as the server may read or write them."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, window_us: int = 200, max_batch: int = 256, lanes: int = 3,
+    def __init__(self, hbm_budget_bytes: int = 0, window_us: int = 200, max_batch: int = 64, lanes: int = 3,
                  sigma: int = 14):
         L = lib()
         _server_sigs(L)
@@ -657,3 +668,36 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def plain_requests(plans, views, perms, req_mat, xs, ys, stream=None):
+    """mr_plain_requests: the requests one at a time (H2D, permute, MERBIT
+    SpMV, un-permute, D2H, synchronise). plans / views / perms (device
+    tensors perm[old] = new) per matrix; req_mat, xs, ys per request (host
+    float32 arrays). Returns (elapsed_ms, per-request latencies in us)."""
+    L = lib()
+    _server_sigs(L)
+    k = len(plans)
+    ph = (C.c_void_p * k)(*[p.h.value for p in plans])
+    vv = (CsrView * k)(*views)
+    pp = (C.c_void_p * k)(*[_ptr(t) for t in perms])
+    req = np.ascontiguousarray(req_mat, np.int32)
+    xp = (C.c_void_p * req.size)(*[a.ctypes.data for a in xs])
+    yp = (C.c_void_p * req.size)(*[a.ctypes.data for a in ys])
+    lat = np.zeros(req.size, np.float64)
+    ms = C.c_double(0)
+    check(L.mr_plain_requests(k, ph, vv, pp, req.size, req.ctypes.data, xp, yp, _stream(stream), C.byref(ms),
+                              lat.ctypes.data), "mr_plain_requests")
+    return ms.value, lat
+
+
+def gather_ceiling(colidx, vals, x, reps: int = 20, stream=None) -> float:
+    """mr_gather_ceiling: ms per pass of the gather-only probe over (colidx,
+    vals) device tensors and x."""
+    L = lib()
+    _sig(L.mr_gather_ceiling, C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32,
+         C.POINTER(C.c_float), C.c_void_p)
+    ms = C.c_float(0)
+    check(L.mr_gather_ceiling(_ptr(colidx), _ptr(vals), colidx.numel(), _ptr(x), reps, C.byref(ms), _stream(stream)),
+          "mr_gather_ceiling")
+    return ms.value

@@ -43,6 +43,10 @@ def test_null_arguments_rejected_without_gpu(M):
     rect = M.CsrView(4, 5, 10, 1, 1, 1, 0)
     assert L.mr_permute_csr(C.byref(rect), 1, 1, 1, 1, None) == M.MR_ERR_INVALID_ARG
     assert L.mr_predict_speedup(7, None, None) == M.MR_ERR_INVALID_ARG
+    raw = C.CDLL(M.LIBMR_PATH)
+    assert raw.mr_gather_ceiling(None, None, C.c_int64(1000), None, 5, None, None) == M.MR_ERR_INVALID_ARG
+    assert raw.mr_plain_requests(0, None, None, None, C.c_int64(0), None, None, None, None, None,
+                                 None) == M.MR_ERR_INVALID_ARG
 
 
 def test_pgorder_rejects_bad_input(M):

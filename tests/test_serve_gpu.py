@@ -76,18 +76,61 @@ def test_lru_eviction_under_tight_budget(M, O, pool):
     sizes = [m["reordered"][1].size * 8 + m["perm"].size * 16 for m in pool]
     srv = M.Server(hbm_budget_bytes=int(sum(sorted(sizes)[-2:]) * 1.3), window_us=100, lanes=2)
     ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
-    outs = []
+    # one request at a time, cycling over a pool larger than the budget: with
+    # LRU every matrix is evicted before it is used again
     for rnd in range(3):
         for j, m in enumerate(pool):
             x = M.uniform(m["perm"].size, seed=rnd * 10 + j)
             y = np.empty_like(x)
-            outs.append((j, x, y, srv.submit(ids[j], x, y)))
-    for j, x, y, t in outs:
-        assert srv.wait(t)[0] == M.MR_OK
-        rp, ci, v = pool[j]["orig"]
-        assert _rel(y, O.spmv_f64(rp, ci, v, x)) <= 1e-5
+            assert srv.wait(srv.submit(ids[j], x, y))[0] == M.MR_OK
+            rp, ci, v = pool[j]["orig"]
+            assert _rel(y, O.spmv_f64(rp, ci, v, x)) <= 1e-5
     st = srv.stats()
     assert st["evictions"] > 0 and st["admissions"] > len(pool)
+    assert st["resident_bytes"] <= int(sum(sorted(sizes)[-2:]) * 1.3)
+    srv.close()
+
+
+def test_pinned_and_pageable_vectors_give_identical_results(M, pool):
+    import torch
+    srv = M.Server(window_us=100, lanes=2)
+    ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
+    jobs = []
+    for j, m in enumerate(pool):
+        n = m["perm"].size
+        x = M.uniform(n, seed=40 + j)
+        y = np.full(n, np.nan, np.float32)
+        xp = torch.from_numpy(x).pin_memory()
+        yp = torch.full((n,), float("nan")).pin_memory()
+        jobs.append((srv.submit(ids[j], x, y), srv.submit(ids[j], xp.numpy(), yp.numpy()), y, yp, xp))
+    for t_pageable, t_pinned, y, yp, _ in jobs:
+        assert srv.wait(t_pageable)[0] == M.MR_OK and srv.wait(t_pinned)[0] == M.MR_OK
+        assert np.array_equal(y.view(np.int32), yp.numpy().view(np.int32))
+    srv.close()
+
+
+def test_plain_requests_match_server(M, pool):
+    import torch
+    plans, views, perms, keep = [], [], [], []
+    for m in pool:
+        brp, bci, bv = (torch.from_numpy(a).cuda() for a in m["reordered"])
+        A = M.view(brp, bci, bv)
+        plans.append(M.MerbitPlan(A))
+        views.append(A)
+        perms.append(torch.from_numpy(m["perm"]).cuda())
+    req = np.array([0, 3, 1, 1, 4, 2], np.int32)
+    xs = [M.uniform(pool[k]["perm"].size, seed=70 + i) for i, k in enumerate(req)]
+    ys = [np.full(x.size, np.nan, np.float32) for x in xs]
+    ms, lat = M.plain_requests(plans, views, perms, req, xs, ys)
+    assert ms > 0 and lat.size == req.size and (lat > 0).all()
+    srv = M.Server(window_us=100)
+    ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
+    for k, x, y in zip(req, xs, ys):
+        ys2 = np.empty_like(x)
+        assert srv.wait(srv.submit(ids[k], x, ys2))[0] == M.MR_OK
+        # same SpMV (FP32 values, sigma 14) up to the plan's block and hub
+        # cache, which change the summation order only within FP32 rounding
+        assert _rel(ys2, y.astype(np.float64)) <= 1e-6
     srv.close()
 
 
