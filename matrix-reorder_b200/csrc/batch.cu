@@ -62,7 +62,11 @@ __global__ void __launch_bounds__(WARPS * 32)
     for (long long g = (long long)blockIdx.x * WARPS + warp; g < total_tiles; g += stride) {
         const int it = find_item(prefix, count, g);
         const MerbitOperand<V, SIGMA> m = ops[it].m;
-        merbit_tile<V, SIGMA>(m, (int)(g - __ldg(prefix + it)), s_buf[warp], pol);
+        const int tile = (int)(g - __ldg(prefix + it));
+        if (m.gather_mode == 0)  // warp-uniform: the default gather without a per-gather mode test
+            merbit_tile<V, SIGMA, false, false, 0>(m, tile, s_buf[warp], pol);
+        else
+            merbit_tile<V, SIGMA, false, false, -1>(m, tile, s_buf[warp], pol);
     }
 }
 

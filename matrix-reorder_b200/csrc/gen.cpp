@@ -242,7 +242,7 @@ mrg_csr* mrg_chung_lu(int32_t n, double gamma, double mean_deg, int32_t dmin, in
         for (int32_t i = 0; i < n; ++i) t += std::min((double)dmax, std::max((double)dmin, s * std::pow(i + 1.0, ex)));
         return t / n;
     };
-    double lo = 1e-3, hi = (double)dmax * 4;
+    double lo = 1e-3, hi = (double)dmax * (double)n;  // mean_for(hi) = dmax: every mean up to dmax is reachable
     for (int it = 0; it < 80; ++it) {
         double mid = std::sqrt(lo * hi);
         (mean_for(mid) < mean_deg ? lo : hi) = mid;
@@ -289,16 +289,51 @@ mrg_csr* mrg_chung_lu(int32_t n, double gamma, double mean_deg, int32_t dmin, in
         start[(size_t)r + 1] = start[(size_t)r] + deg[(size_t)r];
     }
     std::vector<int32_t> src((size_t)start[(size_t)n]), dst((size_t)start[(size_t)n]);
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int32_t r = 0; r < n; ++r) {
-        uint64_t st = splitmix64(seed ^ ((uint64_t)r << 20) ^ 0xabcdefull);
-        for (int64_t e = start[(size_t)r]; e < start[(size_t)r + 1]; ++e) {
-            st = splitmix64(st);
-            int32_t col = (int32_t)((st >> 32) % (uint64_t)n);
-            double u = (double)(st & 0xffffffffull) * (1.0 / 4294967296.0);
-            if (u >= prob[(size_t)col]) col = alias[(size_t)col];
-            src[(size_t)e] = id[(size_t)r];
-            dst[(size_t)e] = id[(size_t)col];
+    // each row draws its deg distinct columns in proportion to the weights
+    // (without replacement: a heavy row would otherwise collapse onto the
+    // few heaviest columns when duplicates are merged); if rejections stall
+    // (the row needs most of the remaining weight), the rest is drawn
+    // uniformly
+#pragma omp parallel
+    {
+        std::vector<int32_t> table;
+        std::vector<uint32_t> used;
+#pragma omp for schedule(dynamic, 64)
+        for (int32_t r = 0; r < n; ++r) {
+            const int64_t d = std::min<int64_t>(deg[(size_t)r], n);
+            const int64_t e0 = start[(size_t)r];
+            if (d <= 0) continue;
+            size_t cap = 16;
+            while (cap < (size_t)(2 * d)) cap <<= 1;
+            if (table.size() < cap) table.assign(cap, -1);
+            const int shift = 64 - __builtin_ctzll((unsigned long long)cap);
+            used.clear();
+            auto insert = [&](int32_t c) {
+                size_t h = (size_t)(((uint64_t)(uint32_t)c * 0x9E3779B97F4A7C15ull) >> shift);
+                while (table[h] != -1) {
+                    if (table[h] == c) return false;
+                    h = (h + 1) & (cap - 1);
+                }
+                table[h] = c;
+                used.push_back((uint32_t)h);
+                return true;
+            };
+            uint64_t st = splitmix64(seed ^ ((uint64_t)r << 20) ^ 0xabcdefull);
+            int64_t got = 0, tries = 0;
+            const int64_t max_tries = 64 * d + 1024;
+            while (got < d) {
+                st = splitmix64(st);
+                int32_t col = (int32_t)((st >> 32) % (uint64_t)n);
+                if (tries++ < max_tries) {
+                    const double u = (double)(st & 0xffffffffull) * (1.0 / 4294967296.0);
+                    if (u >= prob[(size_t)col]) col = alias[(size_t)col];
+                }
+                if (!insert(col)) continue;
+                src[(size_t)(e0 + got)] = id[(size_t)r];
+                dst[(size_t)(e0 + got)] = id[(size_t)col];
+                ++got;
+            }
+            for (uint32_t h : used) table[h] = -1;
         }
     }
     mrg_csr* m = csr_from_edges(n, src, dst);

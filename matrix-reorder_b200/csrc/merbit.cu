@@ -144,14 +144,14 @@ int launch_merbit_plan(const int* rowptr, int nrow, int nnz, int sigma, int lane
 
 // ----------------------------------------------------------------- SpMV ----
 
-template <typename V, int SIGMA, int WARPS>
+template <typename V, int SIGMA, int WARPS, int GM>
 __global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOperand<V, SIGMA> m, int tile_num)
 {
     __shared__ __align__(16) float s_buf[WARPS][tile_smem_words<SIGMA>()];
     const int warp = threadIdx.x >> 5;
     const int tile = blockIdx.x * WARPS + warp;
     if (tile >= tile_num) return;
-    merbit_tile<V, SIGMA>(m, tile, s_buf[warp], TilePolicy{l2_evict_last_policy(), 0});
+    merbit_tile<V, SIGMA, false, false, GM>(m, tile, s_buf[warp], TilePolicy{l2_evict_last_policy(), 0});
 }
 
 // ---- persistent form: one CTA of 32 warps per SM sweeps a contiguous chunk
@@ -205,7 +205,7 @@ __device__ __forceinline__ void fixup_boundary(const uint32_t* __restrict__ tile
     y[R] = (float)((double)__ldcg(y + R) + acc);
 }
 
-template <typename V, int SIGMA, bool HUB>
+template <typename V, int SIGMA, bool HUB, int GM>
 __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     merbit_persistent_kernel(const MerbitOperand<V, SIGMA> m_in, int tile_num, int nrow, int* __restrict__ ticket,
                              const int32_t* __restrict__ hub_cols, int hub_k)
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
         m.hub = hub;
         __syncthreads();
     }
-    for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true, HUB>(m, t, s, pol);
+    for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true, HUB, GM>(m, t, s, pol);
     __syncthreads();
     for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x) fixup_in_chunk(m.tile_y, m.carry, t0, t1, nrow, m.y, t);
     __threadfence();
@@ -286,7 +286,12 @@ static int launch_spmv_t(const MerbitPlan& p, const int* colidx, const void* val
     m.vec_ok = vec_ok;
     m.hub = nullptr;
     m.gather_mode = p.gather_mode;
-    if (grid > 0) merbit_spmv_kernel<V, SIGMA, WARPS><<<grid, WARPS * 32, 0, st>>>(m, p.tile_num);
+    if (grid > 0) {
+        if (p.gather_mode == 0)
+            merbit_spmv_kernel<V, SIGMA, WARPS, 0><<<grid, WARPS * 32, 0, st>>>(m, p.tile_num);
+        else
+            merbit_spmv_kernel<V, SIGMA, WARPS, -1><<<grid, WARPS * 32, 0, st>>>(m, p.tile_num);
+    }
     MR_CUDA_TRY(cudaGetLastError());
     if (p.tile_num > 0) {
         merbit_fixup_kernel<<<(p.tile_num + 255) / 256, 256, 0, st>>>(p.tile_y, carry, p.tile_num, p.n_rows, y);
@@ -295,7 +300,7 @@ static int launch_spmv_t(const MerbitPlan& p, const int* colidx, const void* val
     return MR_OK;
 }
 
-template <typename V, int SIGMA>
+template <typename V, int SIGMA, int GM>
 static int launch_persistent(const MerbitPlan& p, const int* colidx, const void* vals, int nnz, const float* x,
                              float* y, float* carry, cudaStream_t st)
 {
@@ -328,35 +333,35 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
             cudaFuncAttributes fa;
-            cfg = cudaFuncGetAttributes(&fa, merbit_persistent_kernel<V, SIGMA, true>);
+            cfg = cudaFuncGetAttributes(&fa, merbit_persistent_kernel<V, SIGMA, true, GM>);
             // static and dynamic shared memory together may not exceed the opt-in limit
             if (cfg == cudaSuccess)
-                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true>,
+                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true, GM>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            optin - (int)fa.sharedSizeBytes);
         });
         MR_CUDA_TRY(cfg);
         // carve-out sized to this plan's shared memory: the rest stays L1
         const int pct = std::min(100, (int)((smem + 1023) / 1024 * 100 / 228) + 1);
-        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true>,
+        MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true, GM>,
                                          cudaFuncAttributePreferredSharedMemoryCarveout, pct));
-        merbit_persistent_kernel<V, SIGMA, true><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows,
+        merbit_persistent_kernel<V, SIGMA, true, GM><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows,
                                                                                         p.ticket, p.hub_cols, p.hub_k);
     } else {
         static std::once_flag once;
         static cudaError_t cfg = cudaSuccess;
         std::call_once(once, [&] {
-            cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false>,
+            cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false, GM>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
             // smallest shared-memory carve-out that fits: the rest of the
             // SM's 256 KB stays L1 for x
             const int pct = (int)((stage + 1023) / 1024 * 100 / 228) + 1;
             if (cfg == cudaSuccess)
-                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false>,
+                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false, GM>,
                                            cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100));
         });
         MR_CUDA_TRY(cfg);
-        merbit_persistent_kernel<V, SIGMA, false><<<grid, kPersistWarps * 32, stage, st>>>(m, p.tile_num, p.n_rows,
+        merbit_persistent_kernel<V, SIGMA, false, GM><<<grid, kPersistWarps * 32, stage, st>>>(m, p.tile_num, p.n_rows,
                                                                                           p.ticket, nullptr, 0);
     }
     MR_CUDA_TRY(cudaGetLastError());
@@ -502,7 +507,9 @@ static int launch_spmv_w(const MerbitPlan& p, const int* colidx, const void* val
                          float* carry, cudaStream_t st)
 {
     switch (p.block) {
-    case 1024: return launch_persistent<V, SIGMA>(p, colidx, vals, nnz, x, y, carry, st);
+    case 1024:
+        return p.gather_mode == 0 ? launch_persistent<V, SIGMA, 0>(p, colidx, vals, nnz, x, y, carry, st)
+                                  : launch_persistent<V, SIGMA, -1>(p, colidx, vals, nnz, x, y, carry, st);
     case 128: return launch_spmv_t<V, SIGMA, 4>(p, colidx, vals, nnz, x, y, carry, st);
     case 512:
         // 16 warps only while the static staging buffers fit in 48 KB

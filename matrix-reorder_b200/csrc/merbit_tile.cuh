@@ -68,7 +68,22 @@ template <bool NA, typename T> __device__ __forceinline__ T ld_s(const T* p, uin
         return ld_stream(p);
 }
 
-template <typename V, int SIGMA, bool NA = false, bool HUB = false>
+// x[c] for one nonzero. Hub plans mark columns staged in shared memory by the
+// sign bit (slot in the low bits). GM = 0 is the default gather (read-only
+// path, L2 evict-last) fixed at compile time, so the hot path has no mode
+// test per gather; GM = -1 reads m.gather_mode (the plan's tuning flags).
+template <bool HUB, int GM, typename V, int SIGMA>
+__device__ __forceinline__ float gather_x(const MerbitOperand<V, SIGMA>& m, int c, uint64_t pol)
+{
+    if constexpr (HUB)
+        if (c < 0) return m.hub[c & 0x7fffffff];
+    if constexpr (GM == 0)
+        return ld_x(m.x + c, pol);
+    else
+        return ld_x_mode(m.x + c, pol, m.gather_mode);
+}
+
+template <typename V, int SIGMA, bool NA = false, bool HUB = false, int GM = 0>
 __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, const int tile, float* __restrict__ s,
                                             const TilePolicy pols)
 {
@@ -136,16 +151,18 @@ __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, co
             if (v < nvec) {
                 const int k = a0 + 4 * v;
                 float p[4];
+                if (!single_row) {
+                    // products outside [x0, x1) land in staging slots that
+                    // the walk never reads: no per-element range test. Their
+                    // column indices are real entries of neighbouring tiles
+                    // (vector path) or 0 (edge path), so every gather is in
+                    // bounds.
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    p[j] = 0.f;
-                    if (k + j >= x0 && k + j < x1) {
-                        const int c = col[u][j];
-                        if constexpr (HUB)  // hub columns carry the sign bit and read shared memory
-                            p[j] = val[u][j] * ((c < 0) ? m.hub[c & 0x7fffffff] : ld_x_mode(m.x + c, pol, m.gather_mode));
-                        else
-                            p[j] = val[u][j] * ld_x_mode(m.x + c, pol, m.gather_mode);
-                    }
+                    for (int j = 0; j < 4; ++j) p[j] = val[u][j] * gather_x<HUB, GM>(m, col[u][j], pol);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        p[j] = (k + j >= x0 && k + j < x1) ? val[u][j] * gather_x<HUB, GM>(m, col[u][j], pol) : 0.f;
                 }
                 if (single_row)
                     part += (p[0] + p[1]) + (p[2] + p[3]);
