@@ -185,7 +185,8 @@ struct Lane {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     PinnedVec<float> hx, hy;
-    DevVec dx, dxp, dyp, dy, carry, ops, prefix, pops, pprefix;
+    PinnedVec<unsigned char> meta_h;  // the batch's small tables, one DMA per batch
+    DevVec dx, dxp, dyp, dy, carry, meta_d;
     std::vector<Request*> reqs;
     std::vector<long long> off;
     std::vector<int> mats;
@@ -341,16 +342,23 @@ int launch_batch(mr_server* s, Lane& L)
         carry_total += std::max(m.plan.tile_num, 1);
     }
     MR_TRY(L.carry.reserve(sizeof(float) * (size_t)carry_total, L.st));
+    // the small tables (batch operands per group, tile prefixes, permutation
+    // operands) live in one pinned block per lane and go over in one copy:
+    // a pageable source could make the copy wait for the lane's stream
+    auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
     size_t ops_bytes = 0;
-    for (auto& g : groups) ops_bytes += batch_op_bytes(g.first.second, g.first.first) * g.second.size() + 256;
-    MR_TRY(L.ops.reserve(ops_bytes, L.st));
-    MR_TRY(L.prefix.reserve(sizeof(long long) * ((size_t)count + groups.size() * 2 + 2), L.st));
-    MR_TRY(L.pops.reserve(sizeof(PermOp) * (size_t)count, L.st));
-    MR_TRY(L.pprefix.reserve(sizeof(long long) * ((size_t)count + 1), L.st));
-    // host tables, copied with the vectors (pinned staging after the y area)
-    std::vector<unsigned char> ops_host(ops_bytes);
-    std::vector<long long> prefix_host;
-    std::vector<PermOp> pops((size_t)count);
+    for (auto& g : groups) ops_bytes += a256(batch_op_bytes(g.first.second, g.first.first) * g.second.size());
+    const size_t at_prefix = ops_bytes;
+    const size_t at_pops = at_prefix + a256(sizeof(long long) * ((size_t)count + groups.size()));
+    const size_t at_pprefix = at_pops + a256(sizeof(PermOp) * (size_t)count);
+    const size_t meta_bytes = at_pprefix + sizeof(long long) * ((size_t)count + 1);
+    MR_TRY(L.meta_h.reserve(meta_bytes));
+    MR_TRY(L.meta_d.reserve(meta_bytes, L.st));
+    unsigned char* mh = L.meta_h.p;
+    unsigned char* md = static_cast<unsigned char*>(L.meta_d.p);
+    long long* prefix_host = reinterpret_cast<long long*>(mh + at_prefix);
+    size_t n_prefix = 0;
+    PermOp* pops = reinterpret_cast<PermOp*>(mh + at_pops);
     float* dx = static_cast<float*>(L.dx.p);
     float* dxp = static_cast<float*>(L.dxp.p);
     float* dyp = static_cast<float*>(L.dyp.p);
@@ -366,16 +374,16 @@ int launch_batch(mr_server* s, Lane& L)
     for (auto& g : groups) {
         const int sigma = g.first.first, dtype = g.first.second;
         const size_t ob = batch_op_bytes(dtype, sigma);
-        GroupLaunch x{dtype, sigma, (int)g.second.size(), at, prefix_host.size(), 0};
-        prefix_host.push_back(0);
+        GroupLaunch x{dtype, sigma, (int)g.second.size(), at, n_prefix, 0};
+        prefix_host[n_prefix++] = 0;
         for (int i : g.second) {
             const Matrix& m = *L.mp[(size_t)i];
             const mr_csr_view A{m.n, m.n, m.nnz, m.d_rowptr, m.d_colidx, m.d_vals, m.dtype};
-            MR_TRY(batch_fill_op(ops_host.data() + at, dtype, sigma, m.plan, A, dxp + L.off[(size_t)i],
-                                 dyp + L.off[(size_t)i], carry + carry_off[(size_t)i]));
+            MR_TRY(batch_fill_op(mh + at, dtype, sigma, m.plan, A, dxp + L.off[(size_t)i], dyp + L.off[(size_t)i],
+                                 carry + carry_off[(size_t)i]));
             at += ob;
             x.tiles += m.plan.tile_num;
-            prefix_host.push_back(x.tiles);
+            prefix_host[n_prefix++] = x.tiles;
         }
         at = (at + 255) / 256 * 256;
         gl.push_back(x);
@@ -384,28 +392,23 @@ int launch_batch(mr_server* s, Lane& L)
         const Matrix& m = *L.mp[(size_t)i];
         pops[(size_t)i] = PermOp{m.d_perm, L.off[(size_t)i], m.n};
     }
+    std::memcpy(mh + at_pprefix, L.off.data(), sizeof(long long) * ((size_t)count + 1));
     cudaStream_t st = L.st;
+    MR_CUDA_TRY(cudaMemcpyAsync(md, mh, meta_bytes, cudaMemcpyHostToDevice, st));
     for (int i = 0; i < count; ++i) {
         const Request* r = L.reqs[(size_t)i];
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
         MR_CUDA_TRY(cudaMemcpyAsync(dx + o, r->x_pinned ? r->x : L.hx.p + o, nb, cudaMemcpyHostToDevice, st));
     }
-    // the small tables go through pageable memory; the copy is synchronous
-    // with respect to the host buffer, which is then free to reuse
-    MR_CUDA_TRY(cudaMemcpyAsync(L.ops.p, ops_host.data(), at, cudaMemcpyHostToDevice, st));
-    MR_CUDA_TRY(cudaMemcpyAsync(L.prefix.p, prefix_host.data(), sizeof(long long) * prefix_host.size(),
-                                cudaMemcpyHostToDevice, st));
-    MR_CUDA_TRY(cudaMemcpyAsync(L.pops.p, pops.data(), sizeof(PermOp) * (size_t)count, cudaMemcpyHostToDevice, st));
-    MR_CUDA_TRY(cudaMemcpyAsync(L.pprefix.p, L.off.data(), sizeof(long long) * (size_t)count, cudaMemcpyHostToDevice,
-                                st));
     const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 8));
-    const PermOp* d_pops = static_cast<const PermOp*>(L.pops.p);
-    const long long* d_pprefix = static_cast<const long long*>(L.pprefix.p);
+    const PermOp* d_pops = reinterpret_cast<const PermOp*>(md + at_pops);
+    const long long* d_pprefix = reinterpret_cast<const long long*>(md + at_pprefix);
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dx, dxp, 0);
     MR_CUDA_TRY(cudaGetLastError());
     for (const auto& g : gl)
-        MR_TRY(batch_launch_ops(g.dtype, g.sigma, static_cast<unsigned char*>(L.ops.p) + g.ops_at,
-                                static_cast<const long long*>(L.prefix.p) + g.prefix_at, g.count, g.tiles, st));
+        MR_TRY(batch_launch_ops(g.dtype, g.sigma, md + g.ops_at,
+                                reinterpret_cast<const long long*>(md + at_prefix) + g.prefix_at, g.count, g.tiles,
+                                st));
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
     MR_CUDA_TRY(cudaGetLastError());
     for (int i = 0; i < count; ++i) {
@@ -767,7 +770,7 @@ int mr_server_destroy(mr_server* s)
     for (auto& m : s->mats)
         if (m->resident) free_resident(*m, s->admit_st);
     for (auto& L : s->lanes) {
-        for (DevVec* d : {&L.dx, &L.dxp, &L.dyp, &L.dy, &L.carry, &L.ops, &L.prefix, &L.pops, &L.pprefix})
+        for (DevVec* d : {&L.dx, &L.dxp, &L.dyp, &L.dy, &L.carry, &L.meta_d})
             if (d->p) cudaFreeAsync(d->p, s->admit_st);
         if (L.done) cudaEventDestroy(L.done);
         if (L.st) cudaStreamDestroy(L.st);

@@ -611,6 +611,7 @@ class Server:
         check(L.mr_server_create(C.byref(cfg), C.byref(h)), "mr_server_create")
         self.h = h
         self._keep = []
+        self._inflight = {}  # ticket -> (x, y): the server reads x / writes y until the request ends
 
     def add_matrix(self, rowptr, colidx, vals, perm_old2new=None) -> int:
         rowptr = np.ascontiguousarray(rowptr, np.int32)
@@ -633,15 +634,19 @@ class Server:
     def submit(self, mid: int, x: np.ndarray, y: np.ndarray) -> int:
         t = C.c_uint64(0)
         check(lib().mr_server_submit(self.h, mid, x.ctypes.data, y.ctypes.data, C.byref(t)), "mr_server_submit")
+        self._inflight[t.value] = (x, y)
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 10000):
         lat = C.c_double(0)
         rc = lib().mr_server_wait(self.h, ticket, timeout_ms, C.byref(lat))
+        if rc != MR_ERR_TIMEOUT:
+            self._inflight.pop(ticket, None)
         return rc, lat.value
 
     def drain(self, timeout_ms: int = 60000):
         check(lib().mr_server_drain(self.h, timeout_ms), "mr_server_drain")
+        self._inflight.clear()
 
     def stats(self) -> dict:
         st = ServerStats()
