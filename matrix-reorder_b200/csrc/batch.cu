@@ -50,23 +50,39 @@ __device__ __forceinline__ int find_item(const long long* __restrict__ prefix, i
     return lo;
 }
 
-template <typename V, int SIGMA, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
+// One 1024-thread CTA per SM; CTA b sweeps the contiguous chunk b of the
+// concatenated tile space, its warps taking every 32nd tile, so the warps of
+// an SM work on neighbouring tiles of the same item (x reuse in L1, the
+// streams bypass L1 and leave L2 first). A warp looks its item up again only
+// when its tile leaves the current item.
+constexpr int kBatchWarps = 32;
+
+template <typename V, int SIGMA>
+__global__ void __launch_bounds__(kBatchWarps * 32, 1)
     batch_spmv_kernel(const BatchOp<V, SIGMA>* __restrict__ ops, const long long* __restrict__ prefix, int count,
                       long long total_tiles)
 {
-    __shared__ __align__(16) float s_buf[WARPS][tile_smem_words<SIGMA>()];
+    extern __shared__ __align__(16) float s_dyn[];
     const int warp = threadIdx.x >> 5;
-    const TilePolicy pol{l2_evict_last_policy(), 0};
-    const long long stride = (long long)gridDim.x * WARPS;
-    for (long long g = (long long)blockIdx.x * WARPS + warp; g < total_tiles; g += stride) {
-        const int it = find_item(prefix, count, g);
-        const MerbitOperand<V, SIGMA> m = ops[it].m;
-        const int tile = (int)(g - __ldg(prefix + it));
+    float* s = s_dyn + warp * tile_smem_words<SIGMA>();
+    const TilePolicy pol{l2_evict_last_policy(), l2_evict_first_policy()};
+    const long long chunk = (total_tiles + gridDim.x - 1) / gridDim.x;
+    const long long g0 = min64((long long)blockIdx.x * chunk, total_tiles);
+    const long long g1 = min64(g0 + chunk, total_tiles);
+    int it = 0;
+    long long lo = 0, hi = 0;
+    for (long long g = g0 + warp; g < g1; g += kBatchWarps) {
+        if (g < lo || g >= hi) {
+            it = find_item(prefix, count, g);
+            lo = __ldg(prefix + it);
+            hi = __ldg(prefix + it + 1);
+        }
+        const MerbitOperand<V, SIGMA>& m = ops[it].m;  // fields read where used (registers are scarce)
+        const int tile = (int)(g - lo);
         if (m.gather_mode == 0)  // warp-uniform: the default gather without a per-gather mode test
-            merbit_tile<V, SIGMA, false, false, 0>(m, tile, s_buf[warp], pol);
+            merbit_tile<V, SIGMA, true, false, 0>(m, tile, s, pol);
         else
-            merbit_tile<V, SIGMA, false, false, -1>(m, tile, s_buf[warp], pol);
+            merbit_tile<V, SIGMA, true, false, -1>(m, tile, s, pol);
     }
 }
 
@@ -89,7 +105,6 @@ __global__ void batch_fixup_kernel(const BatchOp<V, SIGMA>* __restrict__ ops, co
 
 namespace {
 
-constexpr int kBatchWarps = 8;
 
 struct Group {
     int sigma = 14;
@@ -134,8 +149,19 @@ int launch_group_t(const Group& g, cudaStream_t st)
 {
     if (g.total_tiles == 0) return MR_OK;
     const auto* ops = reinterpret_cast<const BatchOp<V, SIGMA>*>(g.ops);
-    batch_spmv_kernel<V, SIGMA, kBatchWarps><<<g.grid, kBatchWarps * 32, 0, st>>>(ops, g.prefix, (int)g.items.size(),
-                                                                                 g.total_tiles);
+    const size_t smem = sizeof(float) * (size_t)kBatchWarps * tile_smem_words<SIGMA>();
+    static std::once_flag once;
+    static cudaError_t cfg = cudaSuccess;
+    std::call_once(once, [&] {
+        cfg = cudaFuncSetAttribute(batch_spmv_kernel<V, SIGMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        // smallest shared-memory carve-out that fits: the rest stays L1 for x
+        if (cfg == cudaSuccess)
+            cfg = cudaFuncSetAttribute(batch_spmv_kernel<V, SIGMA>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       std::min(100, (int)((smem + 1023) / 1024 * 100 / 228) + 1));
+    });
+    MR_CUDA_TRY(cfg);
+    batch_spmv_kernel<V, SIGMA><<<g.grid, kBatchWarps * 32, smem, st>>>(ops, g.prefix, (int)g.items.size(),
+                                                                       g.total_tiles);
     MR_CUDA_TRY(cudaGetLastError());
     const int fg = (int)std::max<long long>(1, std::min<long long>((g.total_tiles + 255) / 256, sm_count() * 8));
     batch_fixup_kernel<V, SIGMA><<<fg, 256, 0, st>>>(ops, g.prefix, (int)g.items.size(), g.total_tiles);
@@ -211,7 +237,7 @@ int batch_launch_ops(int dtype, int sigma, const void* d_ops, const long long* d
     g.prefix = const_cast<long long*>(d_prefix);
     g.total_tiles = total_tiles;
     g.grid = (int)std::max<long long>(
-        1, std::min<long long>((total_tiles + kBatchWarps - 1) / kBatchWarps, (long long)sm_count() * 4));
+        1, std::min<long long>((total_tiles + kBatchWarps - 1) / kBatchWarps, (long long)sm_count()));
     const int rc = dispatch(dtype, sigma, LaunchF{&g, st});
     g.ops = nullptr;
     g.prefix = nullptr;
@@ -307,7 +333,7 @@ int mr_batch_create(const mr_batch_item* items, int32_t count, void* stream, mr_
         }
         g.total_tiles = prefix[(size_t)n];
         g.grid = (int)std::max<long long>(
-            1, std::min<long long>((g.total_tiles + kBatchWarps - 1) / kBatchWarps, (long long)sm_count() * 4));
+            1, std::min<long long>((g.total_tiles + kBatchWarps - 1) / kBatchWarps, (long long)sm_count()));
         if (cudaMalloc(&g.ops, std::max<size_t>(g.host_ops.size(), 16)) != cudaSuccess ||
             cudaMalloc(&g.prefix, sizeof(long long) * prefix.size()) != cudaSuccess) {
             cudaGetLastError();

@@ -431,9 +431,12 @@ int hub_capacity(int sigma)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const long long stage = 4ll * kPersistWarps * (32 * sigma + 8);
-    // leave 64 KB of the SM's memory as L1: the x gathers that miss the hub
-    // cache need it (measured on R-MAT s22: below ~40 KB of L1 the kernel
-    // slows down by a third whatever the hub coverage)
+    // leave 64 KB of the SM's memory as L1. The x gathers that miss the hub
+    // hit L1 only ~2% of the time, but every load in flight holds L1 space:
+    // on R-MAT s22 (SIGMA 20) a 32 KB reserve costs a third of the
+    // throughput although the larger hub serves 50% instead of 44% of the
+    // gathers, and a smaller hub (more L1) is slower again (-1% at 16K
+    // columns, -7% at 4K)
     const long long room = (long long)optin - stage - 65536 - 1024;
     if (room <= 0) return 0;
     return (int)std::min<long long>(room / 4 / 128 * 128, 1 << 20);

@@ -55,43 +55,46 @@ using Clock = std::chrono::steady_clock;
 namespace {
 
 struct PermOp {
-    const int32_t* perm;  // nullptr: identity
+    const int32_t* perm;  // perm[old] = new, nullptr: identity
+    const int32_t* n2o;   // n2o[new] = old (the inverse), nullptr: identity
     long long off;        // offset of this item's vector in the batch arena
     int n;
 };
 
-// item owning position g: largest i with prefix[i] <= g
-__device__ __forceinline__ int find_seg(const long long* __restrict__ prefix, int count, long long g)
-{
-    int lo = 0, hi = count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (prefix[mid] <= g)
-            lo = mid;
-        else
-            hi = mid - 1;
-    }
-    return lo;
-}
-
-// inverse == 0: out[off + perm[i]] = in[off + i]; else out[off + i] = in[off + perm[i]]
+// Batched permutation of every item's vector, as a gather on both sides so
+// that the writes are coalesced: inverse == 0 gives x'[j] = x[n2o[j]]
+// (x' = P x), inverse != 0 gives y[i] = y'[perm[i]] (y = P^T y'). Each
+// thread walks a contiguous range of the arena and looks its item up again
+// only when it crosses into the next one.
 __global__ void batch_permute_kernel(const PermOp* __restrict__ ops, const long long* __restrict__ prefix, int count,
                                      long long total, const float* __restrict__ in, float* __restrict__ out,
                                      int inverse)
 {
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-         g += (long long)gridDim.x * blockDim.x) {
-        const PermOp op = ops[find_seg(prefix, count, g)];
-        const int i = (int)(g - op.off);
-        if (!op.perm) {
-            out[g] = in[g];
-        } else {
-            const int p = op.perm[i];
-            if (inverse)
-                out[g] = in[op.off + p];
-            else
-                out[op.off + p] = in[g];
+    const long long nthreads = (long long)gridDim.x * blockDim.x;
+    const long long per = (total + nthreads - 1) / nthreads;
+    // consecutive threads take consecutive elements of a block-sized stripe
+    const long long stripe = (long long)blockDim.x;
+    const long long b0 = (long long)blockIdx.x * blockDim.x * per;
+    const long long b1 = b0 + (long long)blockDim.x * per < total ? b0 + (long long)blockDim.x * per : total;
+    int it = -1;
+    long long lo = 0, hi = 0;
+    const int32_t* idx = nullptr;
+    for (long long g = b0 + threadIdx.x; g < b1; g += stripe) {
+        if (g < lo || g >= hi) {
+            int a = 0, b = count - 1;  // largest item whose offset is <= g
+            while (a < b) {
+                const int mid = (a + b + 1) >> 1;
+                if (__ldg(prefix + mid) <= g)
+                    a = mid;
+                else
+                    b = mid - 1;
+            }
+            it = a;
+            lo = __ldg(prefix + it);
+            hi = it + 1 < count ? __ldg(prefix + it + 1) : total;
+            idx = inverse ? ops[it].perm : ops[it].n2o;
         }
+        out[g] = idx ? __ldg(in + lo + __ldg(idx + (g - lo))) : __ldg(in + g);
     }
 }
 
@@ -135,6 +138,7 @@ struct Matrix {
     int32_t* d_colidx = nullptr;
     void* d_vals = nullptr;
     int32_t* d_perm = nullptr;
+    int32_t* d_n2o = nullptr;  // inverse of d_perm, built at admission
     MerbitPlan plan;
 };
 
@@ -211,6 +215,7 @@ struct mr_server {
     bool stop = false;
     std::thread sched, compl_;
     cudaStream_t admit_st = nullptr;
+    int* d_flag = nullptr;  // device word for launch_perm_invert
     int device = 0;
     // stats
     std::vector<double> lat;
@@ -228,7 +233,7 @@ size_t matrix_bytes(const Matrix& m)
     const int64_t lanes = (items + 13) / 14;
     const int64_t tiles = (lanes + 31) / 32;
     return sizeof(int32_t) * ((size_t)m.n + 1) + (sizeof(int32_t) + dtype_size(m.dtype)) * (size_t)m.nnz +
-           (m.h_perm ? sizeof(int32_t) * (size_t)m.n : 0) + 4 * (size_t)lanes + 8 * (size_t)(tiles + 1) + 1024;
+           (m.h_perm ? 2 * sizeof(int32_t) * (size_t)m.n : 0) + 4 * (size_t)lanes + 8 * (size_t)(tiles + 1) + 1024;
 }
 
 void free_resident(Matrix& m, cudaStream_t st)
@@ -237,10 +242,11 @@ void free_resident(Matrix& m, cudaStream_t st)
     cudaFreeAsync(m.d_colidx, st);
     cudaFreeAsync(m.d_vals, st);
     if (m.d_perm) cudaFreeAsync(m.d_perm, st);
+    if (m.d_n2o) cudaFreeAsync(m.d_n2o, st);
     cudaFreeAsync(m.plan.tile_x, st);
     cudaFreeAsync(m.plan.tile_y, st);
     cudaFreeAsync(m.plan.lane_desc, st);
-    m.d_rowptr = m.d_colidx = m.d_perm = nullptr;
+    m.d_rowptr = m.d_colidx = m.d_perm = m.d_n2o = nullptr;
     m.d_vals = nullptr;
     m.plan.tile_x = m.plan.tile_y = nullptr;
     m.plan.lane_desc = nullptr;
@@ -263,7 +269,7 @@ int make_resident(mr_server* s, Matrix& m)
     m.plan.tile_num = (m.plan.lane_num + 31) / 32;
     const size_t desc_b = m.plan.sigma < 15 ? 4 : 8;
     bool ok = alloc((void**)&m.d_rowptr, 4 * ((size_t)m.n + 1)) && alloc((void**)&m.d_colidx, 4 * (size_t)m.nnz) &&
-              alloc(&m.d_vals, vb * (size_t)m.nnz) && (!m.h_perm || alloc((void**)&m.d_perm, 4 * (size_t)m.n)) &&
+              alloc(&m.d_vals, vb * (size_t)m.nnz) && (!m.h_perm || (alloc((void**)&m.d_perm, 4 * (size_t)m.n) && alloc((void**)&m.d_n2o, 4 * (size_t)m.n))) &&
               alloc((void**)&m.plan.tile_x, 4 * ((size_t)m.plan.tile_num + 1)) &&
               alloc((void**)&m.plan.tile_y, 4 * ((size_t)m.plan.tile_num + 1)) &&
               alloc(&m.plan.lane_desc, desc_b * (size_t)std::max(m.plan.lane_num, 1));
@@ -277,9 +283,15 @@ int make_resident(mr_server* s, Matrix& m)
         cudaMemcpyAsync(m.d_colidx, m.h_colidx, 4 * (size_t)m.nnz, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(m.d_vals, m.h_vals, vb * (size_t)m.nnz, cudaMemcpyHostToDevice, st);
     }
-    if (m.h_perm) cudaMemcpyAsync(m.d_perm, m.h_perm, 4 * (size_t)m.n, cudaMemcpyHostToDevice, st);
-    int rc = launch_merbit_plan(m.d_rowptr, m.n, (int)m.nnz, m.plan.sigma, m.plan.lane_num, m.plan.tile_num,
-                                m.plan.tile_x, m.plan.tile_y, m.plan.lane_desc, st);
+    int rc0 = MR_OK;
+    if (m.h_perm) {
+        cudaMemcpyAsync(m.d_perm, m.h_perm, 4 * (size_t)m.n, cudaMemcpyHostToDevice, st);
+        // the permutation was checked on the host at registration; the flag only satisfies the kernel
+        rc0 = launch_perm_invert(m.n, m.d_perm, m.d_n2o, s->d_flag, st);
+    }
+    int rc = rc0 != MR_OK ? rc0
+                          : launch_merbit_plan(m.d_rowptr, m.n, (int)m.nnz, m.plan.sigma, m.plan.lane_num,
+                                               m.plan.tile_num, m.plan.tile_x, m.plan.tile_y, m.plan.lane_desc, st);
     if (rc == MR_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = MR_ERR_CUDA;
     if (rc != MR_OK) {
         free_resident(m, st);
@@ -390,7 +402,7 @@ int launch_batch(mr_server* s, Lane& L)
     }
     for (int i = 0; i < count; ++i) {
         const Matrix& m = *L.mp[(size_t)i];
-        pops[(size_t)i] = PermOp{m.d_perm, L.off[(size_t)i], m.n};
+        pops[(size_t)i] = PermOp{m.d_perm, m.d_n2o, L.off[(size_t)i], m.n};
     }
     std::memcpy(mh + at_pprefix, L.off.data(), sizeof(long long) * ((size_t)count + 1));
     cudaStream_t st = L.st;
@@ -400,7 +412,7 @@ int launch_batch(mr_server* s, Lane& L)
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
         MR_CUDA_TRY(cudaMemcpyAsync(dx + o, r->x_pinned ? r->x : L.hx.p + o, nb, cudaMemcpyHostToDevice, st));
     }
-    const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 8));
+    const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 4));
     const PermOp* d_pops = reinterpret_cast<const PermOp*>(md + at_pops);
     const long long* d_pprefix = reinterpret_cast<const long long*>(md + at_pprefix);
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dx, dxp, 0);
@@ -574,7 +586,9 @@ int mr_server_create(const mr_server_config* cfg, mr_server** out)
         s->cfg.hbm_budget_bytes = (int64_t)(fr / 2);
     }
     s->lanes.resize((size_t)s->cfg.lanes);
-    bool ok = cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) == cudaSuccess;
+    bool ok = cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(&s->d_flag, sizeof(int)) == cudaSuccess &&
+              cudaMemset(s->d_flag, 0, sizeof(int)) == cudaSuccess;
     for (auto& L : s->lanes)
         ok = ok && cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) == cudaSuccess &&
              cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) == cudaSuccess;
@@ -779,6 +793,7 @@ int mr_server_destroy(mr_server* s)
         cudaStreamSynchronize(s->admit_st);
         cudaStreamDestroy(s->admit_st);
     }
+    if (s->d_flag) cudaFree(s->d_flag);
     for (auto& kv : s->reqs) delete kv.second;
     for (Request* r : s->pending)
         if (s->reqs.find(r->ticket) == s->reqs.end()) delete r;
