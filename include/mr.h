@@ -65,6 +65,11 @@ const char* mr_status_string(int status);
 int mr_version(void);
 /* Last CUDA error text seen by this thread (empty if none). */
 const char* mr_last_error(void);
+/* Temporaries of every entry point come from a per-device stream-ordered
+ * pool that keeps freed memory for the next call (no reference
+ * counterpart). This returns the pool's unused memory of the current device
+ * to the system; later calls grow it again. */
+int mr_release_scratch(void);
 
 /* *valid_host = 1 if rowptr[0] == 0, rowptr is non-decreasing,
  * rowptr[n_rows] == nnz and every column index is in [0, n_cols).

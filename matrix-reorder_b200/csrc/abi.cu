@@ -2,8 +2,10 @@
 // dispatch to the kernels. Declared in include/mr.h.
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -20,6 +22,34 @@ void note_cuda_error(cudaError_t e, const char* what, const char* file, int line
 }
 
 void note_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+cudaMemPool_t scratch_pool()
+{
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)pools.size() <= dev) pools.resize((size_t)dev + 1, nullptr);
+    if (!pools[(size_t)dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;  // callers fall back to the default pool
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[(size_t)dev] = p;
+    }
+    return pools[(size_t)dev];
+}
 
 static int check_view(const mr_csr_view* A, bool need_square)
 {
@@ -58,6 +88,15 @@ const char* mr_status_string(int s)
 }
 
 int mr_version(void) { return 10000; }
+
+int mr_release_scratch(void)
+{
+    cudaMemPool_t p = scratch_pool();
+    if (!p) return MR_ERR_CUDA;
+    MR_CUDA_TRY(cudaDeviceSynchronize());
+    MR_CUDA_TRY(cudaMemPoolTrimTo(p, 0));
+    return MR_OK;
+}
 
 const char* mr_last_error(void) { return g_last_error.c_str(); }
 

@@ -81,6 +81,12 @@ int pgorder_host(int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_
 int32_t pgorder_width(int32_t n, int64_t nnz);
 
 // stream-ordered scratch
+// Stream-ordered pool of the current device for temporaries (DevBuf). It
+// keeps freed memory for reuse instead of returning it at every
+// synchronisation (the default pool's behaviour), so repeated calls do not
+// map their scratch again; mr_release_scratch() trims it.
+cudaMemPool_t scratch_pool();
+
 struct DevBuf {
     void* p = nullptr;
     cudaStream_t st = nullptr;
@@ -95,7 +101,8 @@ struct DevBuf {
     {
         st = s;
         if (bytes == 0) bytes = 16;
-        cudaError_t e = cudaMallocAsync(&p, bytes, s);
+        cudaMemPool_t pool = scratch_pool();
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, s) : cudaMallocAsync(&p, bytes, s);
         if (e != cudaSuccess) {
             p = nullptr;
             cudaGetLastError();

@@ -16,6 +16,7 @@
 // sort in one CTA (<= 4096), or a CTA-wide chunked merge sort through global
 // scratch (longer rows).
 #include <algorithm>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -246,38 +247,61 @@ int validate_csr(const mr_csr_view& A, int* ok, cudaStream_t st)
 
 // --------------------------------------------------------- CSR permute ----
 
-constexpr int kSmallRow = 32;
-constexpr int kMedRow = 4096;
+constexpr int kSmallRow = 32;   // one warp, one key per lane
+constexpr int kWarpRow = 256;   // one warp, up to 8 keys per lane in registers
+constexpr int kMedRow = 4096;   // one CTA, shared-memory bitonic; longer rows: chunks + merge passes
 
 struct PermStats {
     int bad;
     int bad_csr;
     int max_len;
+    int n_warp;
     int n_med;
     int n_large;
     unsigned long long large_total;
 };
 
-// new row lengths, classification of rows into the medium / large lists
+// new row lengths and the lists of rows that need more than one key per
+// lane (warp-aggregated appends: one atomic per warp and list)
 __global__ void row_lengths_kernel(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ inv,
-                                   int32_t* __restrict__ len, PermStats* stats, int32_t* __restrict__ med_list,
-                                   int32_t* __restrict__ large_list)
+                                   int32_t* __restrict__ len, PermStats* stats, int32_t* __restrict__ warp_list,
+                                   int32_t* __restrict__ med_list, int32_t* __restrict__ large_list)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int o = inv[i];
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const int i = base + (int)threadIdx.x;
         int l = 0;
-        if (o >= 0 && o < n) l = rowptr[o + 1] - rowptr[o];
-        len[i] = l;
-        if (l > kSmallRow) {
+        if (i < n) {
+            const int o = inv[i];
+            if (o >= 0 && o < n) l = rowptr[o + 1] - rowptr[o];
+            len[i] = l;
+        }
+        const int cls = (i >= n || l <= kSmallRow) ? 0 : (l <= kWarpRow ? 1 : (l <= kMedRow ? 2 : 3));
+        if (cls == 3) {
             atomicMax(&stats->max_len, l);
-            if (l <= kMedRow) {
-                med_list[atomicAdd(&stats->n_med, 1)] = i;
-            } else {
-                large_list[atomicAdd(&stats->n_large, 1)] = i;
-                atomicAdd(&stats->large_total, (unsigned long long)l);
-            }
+            atomicAdd(&stats->large_total, (unsigned long long)l);
+        }
+#pragma unroll
+        for (int c = 1; c <= 3; ++c) {
+            const unsigned m = __ballot_sync(0xffffffffu, cls == c);
+            if (!m) continue;
+            int* counter = c == 1 ? &stats->n_warp : (c == 2 ? &stats->n_med : &stats->n_large);
+            int32_t* list = c == 1 ? warp_list : (c == 2 ? med_list : large_list);
+            const int leader = __ffs(m) - 1;
+            int b = 0;
+            if (lane == leader) b = atomicAdd(counter, __popc(m));
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (cls == c) list[b + __popc(m & ((1u << lane) - 1u))] = i;
         }
     }
+}
+
+// key = (new column << 32) | position in the source row: unique, so every
+// sort below is deterministic and keeps equal columns in source order
+__device__ __forceinline__ unsigned long long perm_key(const int32_t* __restrict__ perm, const int32_t* __restrict__ colidx,
+                                                       int src, int t)
+{
+    return ((unsigned long long)(uint32_t)__ldg(perm + __ldg(colidx + src + t)) << 32) | (unsigned)t;
 }
 
 template <typename E>
@@ -304,7 +328,7 @@ __global__ void __launch_bounds__(256)
         if (len > kSmallRow || len == 0) continue;
         const int src = rowptr[inv[i]];
         unsigned long long key = ~0ull;
-        if (lane < len) key = ((unsigned long long)(uint32_t)perm[colidx[src + lane]] << 32) | (unsigned)lane;
+        if (lane < len) key = perm_key(perm, colidx, src, lane);
         if (len > 1) {
 #pragma unroll
             for (int k = 2; k <= 32; k <<= 1) {
@@ -321,36 +345,170 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// shared-memory bitonic sort of s[0, P) (P a power of two) by one CTA
-__device__ void cta_bitonic(unsigned long long* s, int P)
+// Bitonic stages j = jtop, jtop/2, ..., 1 of merge size `size` on 32*R
+// keys held by one warp in striped order: key r of lane l is element
+// base + r*32 + l of the network (base: the warp's first element), so the
+// compare directions are those of the whole network. Distances below 32
+// exchange across lanes, larger ones inside a thread's registers.
+template <int R>
+__device__ __forceinline__ void warp_stages(unsigned long long (&k)[R], int lane, int base, int size, int jtop)
 {
-    for (int k = 2; k <= P; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
-                const int i = (t / j) * 2 * j + (t % j);
-                const int p = i + j;
-                const bool up = (i & k) == 0;
-                const unsigned long long a = s[i], b = s[p];
-                if ((a > b) == up) {
-                    s[i] = b;
-                    s[p] = a;
+    constexpr int LOG = R >= 16 ? 8 : (R >= 8 ? 7 : (R >= 4 ? 6 : (R >= 2 ? 5 : 4)));  // log2(32 R) - 1
+#pragma unroll
+    for (int jj = LOG; jj >= 0; --jj) {
+        const int j = 1 << jj;
+        if (j > jtop) continue;
+        if (j >= 32) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int p = r ^ (j >> 5);
+                if (p > r) {
+                    const bool up = ((base + r * 32 + lane) & size) == 0;
+                    const unsigned long long a = k[r], b = k[p];
+                    const bool sw = up ? (a > b) : (a < b);
+                    k[r] = sw ? b : a;
+                    k[p] = sw ? a : b;
                 }
             }
-            __syncthreads();
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const bool up = ((base + r * 32 + lane) & size) == 0;
+                const bool lower = (lane & j) == 0;
+                const unsigned long long o = __shfl_xor_sync(0xffffffffu, k[r], j);
+                k[r] = (lower == up) ? min(k[r], o) : max(k[r], o);
+            }
         }
     }
 }
 
-__device__ __forceinline__ int next_pow2(int v)
+// full bitonic sort of the warp's 32*R keys (as part of a network whose
+// element base is the warp's first)
+template <int R> __device__ __forceinline__ void warp_bitonic(unsigned long long (&k)[R], int lane, int base)
 {
-    int p = 1;
-    while (p < v) p <<= 1;
-    return p;
+#pragma unroll
+    for (int size = 2; size <= 32 * R; size <<= 1) warp_stages<R>(k, lane, base, size, size >> 1);
 }
 
-// rows of length (32, 4096]: one CTA per row (grid-stride over the list)
+// Bitonic sort of 256*R keys by a 256-thread CTA: every warp sorts its 32*R
+// keys in registers, then each merge size above a warp's span runs its long
+// distances through shared memory (s[256*R]) and the rest in registers.
+template <int R>
+__device__ __forceinline__ void cta_bitonic_regs(unsigned long long (&k)[R], unsigned long long* s, int warp, int lane)
+{
+    constexpr int WS = 32 * R;
+    constexpr int P = 8 * WS;
+    const int base = warp * WS;
+    warp_bitonic<R>(k, lane, base);
+#pragma unroll
+    for (int size = 2 * WS; size <= P; size <<= 1) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) s[base + r * 32 + lane] = k[r];
+        __syncthreads();
+        for (int j = size >> 1; j >= WS; j >>= 1) {
+            for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                const int i = (t / j) * 2 * j + (t % j);  // bit j of i clear
+                const int q = i + j;
+                const bool up = (i & size) == 0;
+                const unsigned long long a = s[i], b = s[q];
+                if ((a > b) == up) {
+                    s[i] = b;
+                    s[q] = a;
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) k[r] = s[base + r * 32 + lane];
+        __syncthreads();  // s is rewritten by the next merge size
+        warp_stages<R>(k, lane, base, size, WS >> 1);
+    }
+}
+
+template <typename E, int R>
+__device__ __forceinline__ void warp_row_sort(int len, int src, int dst, const int32_t* __restrict__ colidx,
+                                              const E* __restrict__ vals, const int32_t* __restrict__ perm,
+                                              int32_t* __restrict__ out_col, E* __restrict__ out_val, int lane)
+{
+    unsigned long long k[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = r * 32 + lane;
+        k[r] = t < len ? perm_key(perm, colidx, src, t) : ~0ull;
+    }
+    warp_bitonic<R>(k, lane, 0);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = r * 32 + lane;
+        if (t < len) emit_sorted<E>(k[r], dst + t, src, vals, out_col, out_val);
+    }
+}
+
+// rows of length (32, 256]: one warp per row, 2 to 8 keys per lane (a
+// 16-key network unrolled in the same kernel costs more in instruction
+// fetch than it saves)
 template <typename E>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
+    sort_warp_rows_kernel(const int32_t* __restrict__ list, int count, const int32_t* __restrict__ rowptr,
+                          const int32_t* __restrict__ colidx, const E* __restrict__ vals,
+                          const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
+                          const int32_t* __restrict__ out_rowptr, int32_t* __restrict__ out_col,
+                          E* __restrict__ out_val)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
+        const int i = list[w];
+        const int dst = out_rowptr[i];
+        const int len = out_rowptr[i + 1] - dst;
+        const int src = rowptr[inv[i]];
+        if (len <= 64)
+            warp_row_sort<E, 2>(len, src, dst, colidx, vals, perm, out_col, out_val, lane);
+        else if (len <= 128)
+            warp_row_sort<E, 4>(len, src, dst, colidx, vals, perm, out_col, out_val, lane);
+        else
+            warp_row_sort<E, 8>(len, src, dst, colidx, vals, perm, out_col, out_val, lane);
+    }
+}
+
+// keys [0, cnt) of a row segment (positions start + t), sorted by one CTA
+// with 256*R slots, handed to `sink(t, key)` in order
+template <int R, typename F>
+__device__ __forceinline__ void cta_sort_segment(int cnt, int src, int start, const int32_t* __restrict__ colidx,
+                                                 const int32_t* __restrict__ perm, unsigned long long* s, F&& sink)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long k[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = warp * 32 * R + r * 32 + lane;
+        k[r] = t < cnt ? perm_key(perm, colidx, src, start + t) : ~0ull;
+    }
+    cta_bitonic_regs<R>(k, s, warp, lane);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int t = warp * 32 * R + r * 32 + lane;
+        if (t < cnt) sink(t, k[r]);
+    }
+}
+
+template <typename F>
+__device__ __forceinline__ void cta_sort_any(int cnt, int src, int start, const int32_t* __restrict__ colidx,
+                                             const int32_t* __restrict__ perm, unsigned long long* s, F&& sink)
+{
+    if (cnt <= 512)
+        cta_sort_segment<2>(cnt, src, start, colidx, perm, s, sink);
+    else if (cnt <= 1024)
+        cta_sort_segment<4>(cnt, src, start, colidx, perm, s, sink);
+    else if (cnt <= 2048)
+        cta_sort_segment<8>(cnt, src, start, colidx, perm, s, sink);
+    else
+        cta_sort_segment<16>(cnt, src, start, colidx, perm, s, sink);
+}
+
+// rows of length (256, 4096]: one 256-thread CTA per row (grid-stride over the list)
+template <typename E>
+__global__ void __launch_bounds__(256, 2)
     sort_med_rows_kernel(const int32_t* __restrict__ list, int count, const int32_t* __restrict__ rowptr,
                          const int32_t* __restrict__ colidx, const E* __restrict__ vals,
                          const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
@@ -363,88 +521,145 @@ __global__ void __launch_bounds__(256)
         const int dst = out_rowptr[i];
         const int len = out_rowptr[i + 1] - dst;
         const int src = rowptr[inv[i]];
-        const int P = next_pow2(len);
-        for (int t = threadIdx.x; t < P; t += blockDim.x)
-            s[t] = (t < len) ? (((unsigned long long)(uint32_t)perm[colidx[src + t]] << 32) | (unsigned)t) : ~0ull;
+        // sorted keys back to shared memory, then a coalesced emit
+        cta_sort_any(len, src, 0, colidx, perm, s, [&](int t, unsigned long long key) { s[t] = key; });
         __syncthreads();
-        cta_bitonic(s, P);
         for (int t = threadIdx.x; t < len; t += blockDim.x) emit_sorted<E>(s[t], dst + t, src, vals, out_col, out_val);
         __syncthreads();
     }
 }
 
-// rows longer than 4096: sort 4096-key chunks in shared memory, then merge
-// runs pairwise through two global scratch buffers (merge-path split per
-// thread). One CTA per row.
-template <typename E>
-__global__ void __launch_bounds__(256)
-    sort_large_rows_kernel(const int32_t* __restrict__ list, int count, const int32_t* __restrict__ rowptr,
-                           const int32_t* __restrict__ colidx, const E* __restrict__ vals,
-                           const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
-                           const int32_t* __restrict__ out_rowptr, int32_t* __restrict__ out_col,
-                           E* __restrict__ out_val, unsigned long long* scratch, unsigned long long* scratch_used)
+// ---- rows longer than 4096: sorted 4096-key chunks, then merge passes. All
+// long rows are cut into tiles of 4096 output positions; every kernel below
+// runs one CTA per tile over all long rows at once.
+struct LongRow {
+    int dst, src, len, pad;
+    long long soff;  // offset of the row in the two scratch key buffers
+};
+struct LongTile {
+    int row;    // index into the LongRow table
+    int start;  // first position of the tile in the row (multiple of kMedRow)
+};
+
+__global__ void long_rows_kernel(const int32_t* __restrict__ list, int count, const int32_t* __restrict__ rowptr,
+                                 const int32_t* __restrict__ inv, const int32_t* __restrict__ out_rowptr,
+                                 LongRow* __restrict__ rows)
+{
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < count; r += gridDim.x * blockDim.x) {
+        const int i = list[r];
+        LongRow lr;
+        lr.dst = out_rowptr[i];
+        lr.len = out_rowptr[i + 1] - lr.dst;
+        lr.src = rowptr[inv[i]];
+        lr.pad = 0;
+        lr.soff = 0;
+        rows[r] = lr;
+    }
+}
+
+__global__ void __launch_bounds__(256, 2)
+    long_chunk_sort_kernel(const LongTile* __restrict__ tiles, int ntiles, const LongRow* __restrict__ rows,
+                           const int32_t* __restrict__ colidx, const int32_t* __restrict__ perm,
+                           unsigned long long* __restrict__ A)
 {
     __shared__ unsigned long long s[kMedRow];
-    __shared__ unsigned long long s_off;
-    for (int r = blockIdx.x; r < count; r += gridDim.x) {
-        const int i = list[r];
-        const int dst = out_rowptr[i];
-        const int len = out_rowptr[i + 1] - dst;
-        const int src = rowptr[inv[i]];
-        if (threadIdx.x == 0) s_off = atomicAdd(scratch_used, 2ull * (unsigned long long)len);
-        __syncthreads();
-        unsigned long long* A = scratch + s_off;
-        unsigned long long* B = A + len;
-        __syncthreads();
-        // 1) sorted chunks
-        for (int c0 = 0; c0 < len; c0 += kMedRow) {
-            const int cl = min(kMedRow, len - c0);
-            const int P = next_pow2(cl);
-            for (int t = threadIdx.x; t < P; t += blockDim.x)
-                s[t] = (t < cl) ? (((unsigned long long)(uint32_t)perm[colidx[src + c0 + t]] << 32) |
-                                   (unsigned)(c0 + t))
-                                : ~0ull;
-            __syncthreads();
-            cta_bitonic(s, P);
-            for (int t = threadIdx.x; t < cl; t += blockDim.x) A[c0 + t] = s[t];
-            __syncthreads();
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const LongTile tl = tiles[t];
+        const LongRow R = rows[tl.row];
+        const int cl = min(kMedRow, R.len - tl.start);
+        unsigned long long* out = A + R.soff + tl.start;
+        cta_sort_any(cl, R.src, tl.start, colidx, perm, s, [&](int u, unsigned long long key) { out[u] = key; });
+    }
+}
+
+// One merge pass: runs of width w are merged pairwise, in[] -> out[] (or,
+// on the last pass, straight into the output CSR). Each thread produces 16
+// consecutive outputs of its tile, starting at its merge-path co-rank.
+template <typename E>
+__global__ void __launch_bounds__(256)
+    long_merge_kernel(const LongTile* __restrict__ tiles, int ntiles, const LongRow* __restrict__ rows, int w,
+                      const unsigned long long* __restrict__ in, unsigned long long* __restrict__ out, int last,
+                      const E* __restrict__ vals, int32_t* __restrict__ out_col, E* __restrict__ out_val)
+{
+    constexpr int PER = kMedRow / 256;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const LongTile tl = tiles[t];
+        const LongRow R = rows[tl.row];
+        const int lo = tl.start / (2 * w) * (2 * w);
+        const int mid = min(lo + w, R.len), hi = min(lo + 2 * w, R.len);
+        const int na = mid - lo, nb = hi - mid;
+        const unsigned long long* a = in + R.soff + lo;
+        const unsigned long long* b = in + R.soff + mid;
+        const int d0 = tl.start - lo + (int)threadIdx.x * PER;
+        const int d1 = min(d0 + PER, min(tl.start + kMedRow, R.len) - lo);
+        if (d0 >= d1) continue;
+        // co-rank: how many of the first d0 outputs come from a
+        int alo = max(0, d0 - nb), ahi = min(d0, na);
+        while (alo < ahi) {
+            const int am = (alo + ahi) >> 1;
+            if (a[am] < b[d0 - am - 1])
+                alo = am + 1;
+            else
+                ahi = am;
         }
-        // 2) pairwise merges of runs of width w
-        for (int w = kMedRow; w < len; w <<= 1) {
-            for (int lo = 0; lo < len; lo += 2 * w) {
-                const int mid = min(lo + w, len), hi = min(lo + 2 * w, len);
-                const int na = mid - lo, nb = hi - mid, tot = na + nb;
-                const int per = (tot + blockDim.x - 1) / blockDim.x;
-                const int d0 = min((int)threadIdx.x * per, tot), d1 = min(d0 + per, tot);
-                // co-rank: a elements taken among the first d0 outputs
-                int alo = max(0, d0 - nb), ahi = min(d0, na);
-                while (alo < ahi) {
-                    const int am = (alo + ahi) >> 1;
-                    if (A[lo + am] < A[mid + d0 - am - 1])
-                        alo = am + 1;
-                    else
-                        ahi = am;
-                }
-                int ia = alo, ib = d0 - alo;
-                for (int d = d0; d < d1; ++d) {
-                    const bool takeA = ib >= nb || (ia < na && A[lo + ia] < A[mid + ib]);
-                    B[lo + d] = takeA ? A[lo + ia++] : A[mid + ib++];
-                }
-            }
-            __syncthreads();
-            unsigned long long* t = A;
-            A = B;
-            B = t;
+        int ia = alo, ib = d0 - alo;
+        for (int d = d0; d < d1; ++d) {
+            const bool takeA = ib >= nb || (ia < na && a[ia] < b[ib]);
+            const unsigned long long key = takeA ? a[ia++] : b[ib++];
+            if (last)
+                emit_sorted<E>(key, R.dst + lo + d, R.src, vals, out_col, out_val);
+            else
+                out[R.soff + lo + d] = key;
         }
-        for (int t = threadIdx.x; t < len; t += blockDim.x) emit_sorted<E>(A[t], dst + t, src, vals, out_col, out_val);
-        __syncthreads();
     }
 }
 
 template <typename E>
+static int sort_long_rows(const mr_csr_view& A, const int32_t* perm, const int32_t* inv, const int32_t* out_rowptr,
+                          int32_t* out_col, E* out_val, const PermStats& hs, const int32_t* large, cudaStream_t st)
+{
+    const int nl = hs.n_large;
+    DevBuf rows_d, tiles_d, scratch;
+    MR_TRY(rows_d.alloc(sizeof(LongRow) * (size_t)nl, st));
+    long_rows_kernel<<<grid_for(nl, 256), 256, 0, st>>>(large, nl, A.rowptr, inv, out_rowptr, rows_d.as<LongRow>());
+    MR_CUDA_TRY(cudaGetLastError());
+    std::vector<LongRow> rows((size_t)nl);
+    MR_CUDA_TRY(cudaMemcpyAsync(rows.data(), rows_d.p, sizeof(LongRow) * (size_t)nl, cudaMemcpyDeviceToHost, st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<LongTile> tiles;
+    long long off = 0;
+    for (int r = 0; r < nl; ++r) {
+        rows[(size_t)r].soff = off;
+        off += rows[(size_t)r].len;
+        for (int s0 = 0; s0 < rows[(size_t)r].len; s0 += kMedRow) tiles.push_back(LongTile{r, s0});
+    }
+    const int nt = (int)tiles.size();
+    MR_TRY(tiles_d.alloc(sizeof(LongTile) * (size_t)nt, st));
+    MR_TRY(scratch.alloc(sizeof(unsigned long long) * 2 * (size_t)off, st));
+    // both copies read host vectors that live until the synchronisation below
+    MR_CUDA_TRY(cudaMemcpyAsync(rows_d.p, rows.data(), sizeof(LongRow) * (size_t)nl, cudaMemcpyHostToDevice, st));
+    MR_CUDA_TRY(cudaMemcpyAsync(tiles_d.p, tiles.data(), sizeof(LongTile) * (size_t)nt, cudaMemcpyHostToDevice, st));
+    unsigned long long* bufA = scratch.as<unsigned long long>();
+    unsigned long long* bufB = bufA + off;
+    const int grid = std::min(nt, sm_count() * 8);
+    long_chunk_sort_kernel<<<grid, 256, 0, st>>>(tiles_d.as<LongTile>(), nt, rows_d.as<LongRow>(), A.colidx, perm, bufA);
+    MR_CUDA_TRY(cudaGetLastError());
+    const E* v = reinterpret_cast<const E*>(A.vals);
+    for (int w = kMedRow; w < hs.max_len; w <<= 1) {
+        const int last = 2 * w >= hs.max_len;
+        long_merge_kernel<E><<<grid, 256, 0, st>>>(tiles_d.as<LongTile>(), nt, rows_d.as<LongRow>(), w, bufA, bufB, last,
+                                                 v, out_col, out_val);
+        MR_CUDA_TRY(cudaGetLastError());
+        std::swap(bufA, bufB);
+    }
+    MR_CUDA_TRY(cudaStreamSynchronize(st));  // the host tables above must outlive their copies
+    return MR_OK;
+}
+
+template <typename E>
 static int launch_sorts(const mr_csr_view& A, const int32_t* perm, const int32_t* inv, const int32_t* out_rowptr,
-                        int32_t* out_col, void* out_val, const PermStats& hs, const int32_t* med, const int32_t* large,
-                        cudaStream_t st)
+                        int32_t* out_col, void* out_val, const PermStats& hs, const int32_t* warp_list,
+                        const int32_t* med, const int32_t* large, cudaStream_t st)
 {
     const int n = A.n_rows;
     const E* v = reinterpret_cast<const E*>(A.vals);
@@ -452,20 +667,16 @@ static int launch_sorts(const mr_csr_view& A, const int32_t* perm, const int32_t
     const int grid_small = (int)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)sm_count() * 32);
     sort_small_rows_kernel<E><<<std::max(grid_small, 1), 256, 0, st>>>(n, A.rowptr, A.colidx, v, perm, inv, out_rowptr,
                                                                        out_col, ov);
+    if (hs.n_warp > 0) {
+        const int g = (int)std::min<int64_t>(((int64_t)hs.n_warp * 32 + 255) / 256, (int64_t)sm_count() * 32);
+        sort_warp_rows_kernel<E><<<g, 256, 0, st>>>(warp_list, hs.n_warp, A.rowptr, A.colidx, v, perm, inv, out_rowptr,
+                                                   out_col, ov);
+    }
     if (hs.n_med > 0)
         sort_med_rows_kernel<E><<<std::min(hs.n_med, sm_count() * 8), 256, 0, st>>>(
             med, hs.n_med, A.rowptr, A.colidx, v, perm, inv, out_rowptr, out_col, ov);
     MR_CUDA_TRY(cudaGetLastError());
-    if (hs.n_large > 0) {
-        DevBuf scratch, used;
-        MR_TRY(scratch.alloc(sizeof(unsigned long long) * 2 * (size_t)hs.large_total, st));
-        MR_TRY(used.alloc(sizeof(unsigned long long), st));
-        MR_CUDA_TRY(cudaMemsetAsync(used.p, 0, sizeof(unsigned long long), st));
-        sort_large_rows_kernel<E><<<std::min(hs.n_large, sm_count() * 2), 256, 0, st>>>(
-            large, hs.n_large, A.rowptr, A.colidx, v, perm, inv, out_rowptr, out_col, ov,
-            scratch.as<unsigned long long>(), used.as<unsigned long long>());
-        MR_CUDA_TRY(cudaGetLastError());
-    }
+    if (hs.n_large > 0) MR_TRY(sort_long_rows<E>(A, perm, inv, out_rowptr, out_col, ov, hs, large, st));
     return MR_OK;
 }
 
@@ -480,15 +691,17 @@ int permute_csr(const mr_csr_view& A, const int32_t* perm, int32_t* out_rowptr, 
     DevBuf inv, stats, lists, scan_ws;
     MR_TRY(inv.alloc(sizeof(int32_t) * (size_t)n, st));
     MR_TRY(stats.alloc(sizeof(PermStats), st));
-    MR_TRY(lists.alloc(sizeof(int32_t) * 2 * (size_t)n, st));
+    MR_TRY(lists.alloc(sizeof(int32_t) * 3 * (size_t)n, st));
     MR_TRY(scan_ws.alloc(scan_workspace_bytes(n), st));
     MR_CUDA_TRY(cudaMemsetAsync(stats.p, 0, sizeof(PermStats), st));
     PermStats* ds = stats.as<PermStats>();
     MR_TRY(launch_perm_invert(n, perm, inv.as<int32_t>(), &ds->bad, st));
     MR_TRY(validate_csr_async(A, &ds->bad_csr, st));
-    int32_t* med = lists.as<int32_t>();
+    int32_t* warp_list = lists.as<int32_t>();
+    int32_t* med = warp_list + n;
     int32_t* large = med + n;
-    row_lengths_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, A.rowptr, inv.as<int32_t>(), out_rowptr, ds, med, large);
+    row_lengths_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, A.rowptr, inv.as<int32_t>(), out_rowptr, ds, warp_list, med,
+                                                         large);
     MR_CUDA_TRY(cudaGetLastError());
     MR_TRY(exclusive_scan_i32_ws(out_rowptr, out_rowptr, n, scan_ws.p, st));
     PermStats hs;
@@ -497,8 +710,10 @@ int permute_csr(const mr_csr_view& A, const int32_t* perm, int32_t* out_rowptr, 
     if (hs.bad_csr) return MR_ERR_INVALID_ARG;
     if (hs.bad) return MR_ERR_INVALID_PERM;
     if (A.dtype == MR_F32)
-        return launch_sorts<uint32_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, med, large, st);
-    return launch_sorts<uint16_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, med, large, st);
+        return launch_sorts<uint32_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, warp_list, med,
+                                      large, st);
+    return launch_sorts<uint16_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, warp_list, med,
+                                  large, st);
 }
 
 }  // namespace mr

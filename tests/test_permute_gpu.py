@@ -41,6 +41,17 @@ def _heavy_rows(seed=0):
     return csr_from_dense_pattern(rows)
 
 
+def _duplicate_columns(seed=1):
+    """Rows that repeat column indices, one per sort class (warp, warp x2/4/8
+    keys, CTA, long-row merge): equal new columns must keep source order."""
+    rng = np.random.default_rng(seed)
+    n = 12000
+    rows = [[] for _ in range(n)]
+    for r, k in ((3, 20), (50, 60), (51, 100), (52, 250), (700, 1000), (701, 4096), (9000, 5000), (9001, 11000)):
+        rows[r] = rng.choice(max(k // 3, 2), k, replace=True).tolist()  # unsorted, many repeats
+    return csr_from_dense_pattern(rows)
+
+
 @pytest.fixture(scope="module")
 def mats(M):
     return {
@@ -49,10 +60,11 @@ def mats(M):
         "heavy": _heavy_rows(),
         "random": csr_random(5000, 70, seed=8, empty_frac=0.3),
         "tiny": csr_from_dense_pattern([[1], [0, 1], []]),
+        "dups": _duplicate_columns(),
     }
 
 
-@pytest.mark.parametrize("name", ["rmat14", "lap48", "heavy", "random", "tiny"])
+@pytest.mark.parametrize("name", ["rmat14", "lap48", "heavy", "random", "tiny", "dups"])
 def test_permute_bit_exact_vs_oracle(M, O, mats, name):
     rp, ci, v = mats[name]
     n = rp.size - 1
