@@ -767,8 +767,8 @@ def main() -> int:
     ap.add_argument("--rate", type=float, default=20000.0, help="serve: Poisson arrivals per second")
     ap.add_argument("--seconds", type=float, default=2.0, help="serve: length of the Poisson run")
     ap.add_argument("--window-us", type=int, default=200)
-    ap.add_argument("--max-batch", type=int, default=64)
-    ap.add_argument("--lanes", type=int, default=3)
+    ap.add_argument("--max-batch", type=int, default=32)
+    ap.add_argument("--lanes", type=int, default=6)
     ap.add_argument("--sat-requests", type=int, default=20000)
     ap.add_argument("--plain-requests", type=int, default=2000)
     ap.add_argument("--batch-count", type=int, default=512, help="batch: matrices in the graph launch")

@@ -347,6 +347,30 @@ int mr_predict_speedup(int model, const double* features10, double* speedup);
 int mr_locality_predict(const int32_t* stream_dev, int32_t nnz, int32_t ncols, int32_t graph_id,
                         double* features10, float* speedup, void* stream);
 
+/* ------------------------------------------- predictor-gated reorder ---- */
+
+typedef enum mr_gate {
+    MR_GATE_SKIP = 0,      /* keep the current order */
+    MR_GATE_RELABEL = 1,   /* reorder */
+    MR_GATE_UNCERTAIN = 2  /* inside the band: the caller's policy decides */
+} mr_gate;
+
+/* Band gate of the ridge trainer (run_band_gate_scan, ridge/train.py:983-1026):
+ * RELABEL when predicted >= tau_h, SKIP when predicted <= tau_l (SKIP wins
+ * when both hold), UNCERTAIN otherwise. The trainer scans the pairs
+ * (0.99, 1.01) ... (0.93, 1.07) (BAND_GATE_PAIRS, ridge/train.py:91-99). */
+int mr_band_gate(double predicted_speedup, double tau_l, double tau_h, int32_t* decision);
+
+/* Predicted reorder speedup of an x-access stream (colidx in CSR order) with
+ * ridge model `model` (mr_model): the *_SAMPLED models take the sampled HLL
+ * histogram of GRAPH::locality_predict (src/class.cu:1263-1311, seed from
+ * graph_id), the *_EXACT models the exact histogram
+ * (compute_sector_rd_histogram, src/class.cu:892-936); both with the
+ * reference's 10 bins over 32-column sectors. features10 may be NULL.
+ * Synchronises `stream`; MR_ERR_PREDICT as mr_predict_speedup. */
+int mr_predict_reorder(const int32_t* stream_dev, int32_t nnz, int32_t ncols, int32_t graph_id, int32_t model,
+                       double* features10, double* speedup, void* stream);
+
 /* ------------------------------------------------------------- pGOrder ---- */
 
 /* Partition size of gorder4: GRAPH::get_width (src/class.cu:733-750). */
@@ -379,6 +403,13 @@ int mr_graph_locality_predict(mr_graph* g, double* features10, float* speedup);
  * ms_plan/ms_spmv may be NULL (ms_spmv is per SpMV). */
 int mr_graph_spmv(mr_graph* g, const char* method, int32_t iters, const float* x_host, float* y_host,
                   double* ms_plan, double* ms_spmv);
+/* Predictor-gated reorder (the pipeline sampled RD -> PredictSpeedup -> band
+ * gate -> reorder-or-skip): mr_predict_reorder on the current order with
+ * `model`, mr_band_gate(tau_l, tau_h), then mr_graph_gorder4(vsize, width)
+ * when the gate says RELABEL, or UNCERTAIN and relabel_uncertain != 0.
+ * decision (mr_gate) and predicted may be NULL. */
+int mr_graph_gated_reorder(mr_graph* g, int32_t model, double tau_l, double tau_h, int32_t relabel_uncertain,
+                           int32_t vsize, int32_t width, int32_t* decision, double* predicted);
 /* Current permutation perm[old] = new, and the current device CSR view. */
 int mr_graph_get_perm(const mr_graph* g, int32_t* perm_host);
 int mr_graph_view(const mr_graph* g, mr_csr_view* view);

@@ -297,6 +297,46 @@ int mr_rd_hist_sampled(const int32_t* s, int32_t nnz, int32_t samples, int32_t s
                            status, pos, as_stream(stream));
 }
 
+int mr_band_gate(double predicted, double tau_l, double tau_h, int32_t* decision)
+{
+    if (!decision || !(tau_l == tau_l) || !(tau_h == tau_h)) return MR_ERR_INVALID_ARG;
+    // run_band_gate_scan (ridge/train.py:993-995): "relabel" is set first,
+    // "skip" second, so skip wins when both thresholds hold
+    int32_t d = MR_GATE_UNCERTAIN;
+    if (predicted >= tau_h) d = MR_GATE_RELABEL;
+    if (predicted <= tau_l) d = MR_GATE_SKIP;
+    *decision = d;
+    return MR_OK;
+}
+
+int mr_predict_reorder(const int32_t* s, int32_t nnz, int32_t ncols, int32_t graph_id, int32_t model,
+                       double* features10, double* speedup, void* stream)
+{
+    static const int32_t kEdges[9] = {1, 112, 512, 18432, 36864, 73728, 147456, 294912, 589824};
+    if (!speedup || ncols < 0 || nnz < 0) return MR_ERR_INVALID_ARG;
+    if (model != MR_MODEL_MERBIT_SAMPLED && model != MR_MODEL_MERBIT_EXACT && model != MR_MODEL_CSR_SAMPLED &&
+        model != MR_MODEL_CSR_EXACT)
+        return MR_ERR_INVALID_ARG;
+    double f[10];
+    int64_t counts[10];
+    if (model == MR_MODEL_MERBIT_SAMPLED || model == MR_MODEL_CSR_SAMPLED) {
+        // settings of GRAPH::locality_predict (src/class.cu:1265-1277)
+        int64_t stats[4];
+        MR_TRY(mr_rd_hist_sampled(s, nnz, 30960, 32, kEdges[8], 12, 0, mr_hll_seed(graph_id, 0), kEdges, 9, counts,
+                                  stats, nullptr, nullptr, nullptr, stream));
+        const int64_t valid = stats[0] + stats[2];  // found + large
+        for (int i = 0; i < 10; ++i) f[i] = valid > 0 ? (double)counts[i] / (double)valid : 0.0;
+    } else {
+        // the exact branch of locality_predict (src/class.cu:1284-1298)
+        int64_t valid = 0;
+        MR_TRY(mr_rd_hist_exact(s, nnz, ncols, 32, kEdges, 9, counts, &valid, stream));
+        for (int i = 0; i < 10; ++i) f[i] = valid > 0 ? (double)counts[i] / (double)valid : 0.0;
+    }
+    if (features10)
+        for (int i = 0; i < 10; ++i) features10[i] = f[i];
+    return mr_predict_speedup(model, f, speedup);
+}
+
 int mr_locality_predict(const int32_t* s, int32_t nnz, int32_t ncols, int32_t graph_id, double* features10,
                         float* speedup, void* stream)
 {

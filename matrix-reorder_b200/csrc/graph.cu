@@ -8,7 +8,9 @@
 //   locality_predict (src/class.cu:1263-1326): sampled RD + ridge predictor
 //   spmv(method)     (src/class.cu:1331-1454): "csr" or "merbit" SpMV,
 //                    returning y in the original numbering as the
-//                    reference's check does (src/class.cu:1435-1445).
+//                    reference's check does (src/class.cu:1435-1445),
+// plus the predictor-gated reorder (RD features -> ridge model -> band gate
+// of ridge/train.py:983-1026 -> gorder4 or keep the order).
 #include <chrono>
 #include <cstring>
 #include <new>
@@ -181,6 +183,21 @@ int mr_graph_locality_predict(mr_graph* g, double* features10, float* speedup)
 {
     if (!g) return MR_ERR_INVALID_ARG;
     return mr_locality_predict(g->colidx, (int32_t)g->nnz, g->n, g->graph_id, features10, speedup, g->st);
+}
+
+int mr_graph_gated_reorder(mr_graph* g, int32_t model, double tau_l, double tau_h, int32_t relabel_uncertain,
+                           int32_t vsize, int32_t width, int32_t* decision, double* predicted)
+{
+    if (!g || width < 1) return MR_ERR_INVALID_ARG;
+    double sp = 0.0;
+    MR_TRY(mr_predict_reorder(g->colidx, (int32_t)g->nnz, g->n, g->graph_id, model, nullptr, &sp, g->st));
+    int32_t d = MR_GATE_UNCERTAIN;
+    MR_TRY(mr_band_gate(sp, tau_l, tau_h, &d));
+    if (predicted) *predicted = sp;
+    if (decision) *decision = d;
+    if (d == MR_GATE_RELABEL || (d == MR_GATE_UNCERTAIN && relabel_uncertain))
+        MR_TRY(mr_graph_gorder4(g, vsize, width, nullptr, nullptr));
+    return MR_OK;
 }
 
 int mr_graph_spmv(mr_graph* g, const char* method, int32_t iters, const float* x_host, float* y_host,

@@ -291,6 +291,31 @@ def locality_predict(stream_dev, ncols: int, graph_id: int = 0, stream=None):
 
 # -------------------------------------------------------------- pGOrder ----
 
+GATE_SKIP, GATE_RELABEL, GATE_UNCERTAIN = 0, 1, 2
+# the trainer's scanned (tau_l, tau_h) pairs, ridge/train.py:91-99
+BAND_GATE_PAIRS = [(0.99, 1.01), (0.98, 1.02), (0.97, 1.03), (0.96, 1.04), (0.95, 1.05), (0.94, 1.06), (0.93, 1.07)]
+
+
+def band_gate(predicted: float, tau_l: float, tau_h: float) -> int:
+    L = lib()
+    _sig(L.mr_band_gate, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int32))
+    d = C.c_int32(0)
+    check(L.mr_band_gate(predicted, tau_l, tau_h, C.byref(d)), "mr_band_gate")
+    return d.value
+
+
+def predict_reorder(stream_dev, ncols: int, graph_id: int = 0, model: int = MODEL_MERBIT_SAMPLED, stream=None):
+    """mr_predict_reorder: (predicted speedup, 10 features)."""
+    L = lib()
+    _sig(L.mr_predict_reorder, C.c_int, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_void_p,
+         C.POINTER(C.c_double), C.c_void_p)
+    f = np.zeros(10, np.float64)
+    sp = C.c_double(0)
+    check(L.mr_predict_reorder(_ptr(stream_dev), stream_dev.numel(), ncols, graph_id, model, f.ctypes.data,
+                               C.byref(sp), _stream(stream)), "mr_predict_reorder")
+    return sp.value, f
+
+
 def pgorder_width(n: int, nnz: int) -> int:
     return int(lib().mr_pgorder_width(n, nnz))
 
@@ -337,6 +362,17 @@ class Graph:
         s = C.c_float(0)
         check(lib().mr_graph_locality_predict(self.h, f.ctypes.data, C.byref(s)), "mr_graph_locality_predict")
         return s.value, f
+
+    def gated_reorder(self, model: int = MODEL_MERBIT_SAMPLED, tau_l: float = 0.95, tau_h: float = 1.05,
+                      relabel_uncertain: bool = False, vsize: int = 0, width: int = 5):
+        """mr_graph_gated_reorder: returns (decision, predicted speedup)."""
+        L = lib()
+        _sig(L.mr_graph_gated_reorder, C.c_int, C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32, C.c_int32,
+             C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double))
+        d, p = C.c_int32(0), C.c_double(0)
+        check(L.mr_graph_gated_reorder(self.h, model, tau_l, tau_h, int(relabel_uncertain), vsize, width, C.byref(d),
+                                       C.byref(p)), "mr_graph_gated_reorder")
+        return d.value, p.value
 
     def spmv(self, method: str = "merbit", iters: int = 1, x: Optional[np.ndarray] = None):
         y = np.empty(self.n, np.float32)

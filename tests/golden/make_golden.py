@@ -9,7 +9,11 @@ stores inputs and outputs in tests/golden/golden_host.npz:
   * exact RD bin probabilities (compute_sector_rd_histogram,
     src/class.cu:892-936) for the reference bins and log2 bins,
   * GRAPH::get_width over a grid of sizes (src/class.cu:733-750),
-  * rd_merbit_model::PredictSpeedup on feature vectors (include/model.cuh).
+  * rd_merbit_model::PredictSpeedup on feature vectors (include/model.cuh),
+  * the band gate's decision counts (run_band_gate_scan,
+    ridge/train.py:983-1026, imported from the reference checkout named by
+    MR_REFERENCE, default /root/reference) on seeded predicted / true
+    speedups for every BAND_GATE_PAIRS entry.
 
 Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
 """
@@ -60,6 +64,19 @@ def main() -> None:
     feats = rng.dirichlet(np.ones(10), size=16)
     out["predict_features"] = feats
     out["predict_ref"] = np.array([O.ref_predict(f) for f in feats])
+    # band gate of the ridge trainer, run by the reference's own Python
+    ref = os.environ.get("MR_REFERENCE", "/root/reference")
+    sys.path.insert(0, os.path.join(ref, "ridge"))
+    import pandas as pd
+    import train as T  # the reference's ridge/train.py
+    pred = np.concatenate([rng.lognormal(0.0, 0.05, 400),
+                           np.array([t for pair in T.BAND_GATE_PAIRS for t in pair])])  # exactly on the thresholds
+    true = rng.lognormal(0.0, 0.08, pred.size)
+    scan = T.run_band_gate_scan(pd.DataFrame({"speedup": true, "pred_speedup": pred}), T.BAND_GATE_PAIRS)
+    out["gate_pred"] = pred
+    out["gate_true"] = true
+    out["gate_pairs"] = np.array(T.BAND_GATE_PAIRS, np.float64)
+    out["gate_counts"] = scan[["tp", "tn", "fp", "fn", "num_decided"]].to_numpy(np.int64)
     np.savez_compressed(os.path.join(HERE, "golden_host.npz"), **out)
     print("wrote", os.path.join(HERE, "golden_host.npz"))
 
