@@ -204,6 +204,29 @@ def time_cpu_baseline(brp, bci, bv, xp, budget_s: float = 10.0):
     return spmv_bytes(n, bci.size) * reps / dt / 1e9, used, reps
 
 
+def reference_cpu_functions(rp, ci, bci, n):
+    """The reference's own CPU functions on this path, compiled from its
+    sources into oracle/_ref, timed on the host cores: the exact RD
+    histogram compute_sector_rd_histogram (single-threaded,
+    src/class.cu:892-936) over the reordered x stream, and gorder4's host
+    ordering (order_on_cpu tasks on its ThreadPool(128),
+    src/class.cu:2647-2683) of the original matrix."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as O
+    if not O.ref_available():
+        return None
+    t0 = time.perf_counter()
+    O.ref_rd_probs(bci, n, 32)
+    t_rd = time.perf_counter() - t0
+    vs = O.ref_get_width(n, int(ci.size))
+    t0 = time.perf_counter()
+    O.ref_pgorder(rp, ci, vs, 5)
+    t_pg = time.perf_counter() - t0
+    return {"rd_exact_s": round(t_rd, 2), "rd_exact_threads": 1, "rd_stream_nnz": int(bci.size),
+            "pgorder_s": round(t_pg, 2), "pgorder_pool_threads": 128, "host_cores": os.cpu_count(),
+            "pgorder_vsize": vs}
+
+
 def run_ours(args):
     import torch
     import mrb200 as M
@@ -385,6 +408,9 @@ def run_ours(args):
         cpu = {"value": round(gbs, 2), "unit": "GB/s", "cores": cores, "kind": "port",
                "sample": f"{reps} full FP32 CSR SpMVs of the same reordered matrix (OpenMP restatement; "
                          "the reference has no CPU SpMV)"}
+        ref_fns = reference_cpu_functions(rp, ci, bci_h, n)
+        if ref_fns:
+            cpu["reference_functions"] = ref_fns
 
     plan.close()
     if rank == 0:

@@ -383,6 +383,23 @@ int32_t mr_pgorder_width(int32_t n_rows, int64_t nnz);
 int mr_pgorder(int32_t n, const int32_t* rowptr_host, const int32_t* colidx_host, int32_t vsize,
                int32_t width, int32_t threads, uint32_t* perm_new2old_host);
 
+/* ------------------------------------- other permutation producers ---- */
+
+/* The reference's comparators for pGOrder, on the GPU; each writes
+ * perm[old] = new (n = A->n_rows entries, device) for mr_permute_csr.
+ * Degree of v = number of nonzeros in column v (the reference counts its
+ * row_ind, which holds our column indices). Synchronise `stream`. */
+/* Decreasing degree, ties by increasing id: GRAPH::relabel_degree
+ * (src/class.cu:1493-1549). */
+int mr_order_degree(const mr_csr_view* A, int32_t* perm_old2new_dev, void* stream);
+/* Degree-based grouping: class ceilf(log2(degree + 1.0)) decreasing, ids
+ * increasing within a class: GRAPH::dbg (src/class.cu:1660-1760). */
+int mr_order_dbg(const mr_csr_view* A, int32_t* perm_old2new_dev, void* stream);
+/* A seeded uniform random permutation, standing in for
+ * GRAPH::relabel_random (src/class.cu:1460-1491); not the same permutation
+ * as the reference's thrust::shuffle for the same seed. */
+int mr_order_random(int32_t n, uint32_t seed, int32_t* perm_old2new_dev, void* stream);
+
 /* ------------------------------------------ GRAPH-style host object ---- */
 
 /* A square matrix resident on the device with its current permutation

@@ -81,6 +81,12 @@ int pgorder_host(int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_
 int32_t pgorder_width(int32_t n, int64_t nnz);
 
 // stream-ordered scratch
+// Stable LSD radix sort of (key, value) pairs over the low `bits` bits of the
+// keys, 8 bits per pass, ping-ponging with kbuf / vbuf: on return keys / vals
+// point at the buffers that hold the sorted pairs.
+int radix_sort_pairs_u32(uint32_t*& keys, int32_t*& vals, uint32_t* kbuf, int32_t* vbuf, int64_t n, int bits,
+                         cudaStream_t st);
+
 // Stream-ordered pool of the current device for temporaries (DevBuf). It
 // keeps freed memory for reuse instead of returning it at every
 // synchronisation (the default pool's behaviour), so repeated calls do not

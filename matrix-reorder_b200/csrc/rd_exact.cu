@@ -271,6 +271,26 @@ int grid_of(int64_t n, int threads, int cap_per_sm = 16)
 
 }  // namespace
 
+int radix_sort_pairs_u32(uint32_t*& keys, int32_t*& vals, uint32_t* kbuf, int32_t* vbuf, int64_t n, int bits,
+                         cudaStream_t st)
+{
+    if (n <= 0) return MR_OK;
+    const int tiles = (int)((n + kRsTile - 1) / kRsTile);
+    DevBuf hist, scan_ws;
+    MR_TRY(hist.alloc(sizeof(int32_t) * ((size_t)kRsBuckets * tiles + 1), st));
+    MR_TRY(scan_ws.alloc(scan_workspace_bytes((int64_t)kRsBuckets * tiles), st));
+    for (int shift = 0; shift < bits; shift += 8) {
+        radix_hist_kernel<<<tiles, kRsThreads, 0, st>>>(keys, n, shift, tiles, hist.as<int32_t>());
+        MR_TRY(exclusive_scan_i32_ws(hist.as<int32_t>(), hist.as<int32_t>(), (int64_t)kRsBuckets * tiles, scan_ws.p,
+                                     st));
+        radix_scatter_kernel<<<tiles, kRsThreads, 0, st>>>(keys, vals, n, shift, tiles, hist.as<int32_t>(), kbuf, vbuf);
+        std::swap(keys, kbuf);
+        std::swap(vals, vbuf);
+    }
+    MR_CUDA_TRY(cudaGetLastError());
+    return MR_OK;
+}
+
 int rd_hist_exact(const int32_t* stream, int64_t nnz, int32_t ncols, int32_t sector, const int32_t* edges,
                   int32_t nedges, int64_t* counts, int64_t* valid, cudaStream_t st)
 {
@@ -280,31 +300,20 @@ int rd_hist_exact(const int32_t* stream, int64_t nnz, int32_t ncols, int32_t sec
     const int64_t nsec = ((int64_t)ncols + sector - 1) / sector;
     int bits = 1;
     while (bits < 32 && ((int64_t)1 << bits) < nsec) ++bits;
-    const int tiles = (int)((nnz + kRsTile - 1) / kRsTile);
     const int64_t ms_tiles = (nnz + kMsTile - 1) / kMsTile;
 
-    DevBuf k0, k1, v0, v1, hist, scan_ws, prev, m0, m1, dedges, dcounts;
+    DevBuf k0, k1, v0, v1, prev, m0, m1, dedges, dcounts;
     MR_TRY(k0.alloc(sizeof(uint32_t) * nnz, st));
     MR_TRY(k1.alloc(sizeof(uint32_t) * nnz, st));
     MR_TRY(v0.alloc(sizeof(int32_t) * nnz, st));
     MR_TRY(v1.alloc(sizeof(int32_t) * nnz, st));
-    MR_TRY(hist.alloc(sizeof(int32_t) * ((size_t)kRsBuckets * tiles + 1), st));
-    MR_TRY(scan_ws.alloc(scan_workspace_bytes((int64_t)kRsBuckets * tiles), st));
     MR_TRY(dedges.alloc(sizeof(int32_t) * std::max(nedges, 1), st));
     MR_TRY(dcounts.alloc(sizeof(unsigned long long) * (nedges + 1), st));
 
     sector_keys_kernel<<<grid_of(nnz, 256), 256, 0, st>>>(stream, nnz, sector, k0.as<uint32_t>(), v0.as<int32_t>());
-    uint32_t *ka = k0.as<uint32_t>(), *kb = k1.as<uint32_t>();
-    int32_t *va = v0.as<int32_t>(), *vb = v1.as<int32_t>();
-    for (int shift = 0; shift < bits; shift += 8) {
-        radix_hist_kernel<<<tiles, kRsThreads, 0, st>>>(ka, nnz, shift, tiles, hist.as<int32_t>());
-        MR_TRY(exclusive_scan_i32_ws(hist.as<int32_t>(), hist.as<int32_t>(), (int64_t)kRsBuckets * tiles, scan_ws.p,
-                                     st));
-        radix_scatter_kernel<<<tiles, kRsThreads, 0, st>>>(ka, va, nnz, shift, tiles, hist.as<int32_t>(), kb, vb);
-        std::swap(ka, kb);
-        std::swap(va, vb);
-    }
-    MR_CUDA_TRY(cudaGetLastError());
+    uint32_t* ka = k0.as<uint32_t>();
+    int32_t* va = v0.as<int32_t>();
+    MR_TRY(radix_sort_pairs_u32(ka, va, k1.as<uint32_t>(), v1.as<int32_t>(), nnz, bits, st));
     MR_TRY(prev.alloc(sizeof(int32_t) * nnz, st));
     prev_kernel<<<grid_of(nnz, 256), 256, 0, st>>>(ka, va, nnz, prev.as<int32_t>());
     MR_TRY(m0.alloc(sizeof(int2) * (size_t)ms_tiles * kMsTile, st));

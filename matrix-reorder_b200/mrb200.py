@@ -291,6 +291,25 @@ def locality_predict(stream_dev, ncols: int, graph_id: int = 0, stream=None):
 
 # -------------------------------------------------------------- pGOrder ----
 
+def order_degree(A: CsrView, perm_out, stream=None) -> None:
+    """mr_order_degree: perm_out[old] = new (device int32 tensor)."""
+    L = lib()
+    _sig(L.mr_order_degree, C.c_int, C.POINTER(CsrView), C.c_void_p, C.c_void_p)
+    check(L.mr_order_degree(C.byref(A), _ptr(perm_out), _stream(stream)), "mr_order_degree")
+
+
+def order_dbg(A: CsrView, perm_out, stream=None) -> None:
+    L = lib()
+    _sig(L.mr_order_dbg, C.c_int, C.POINTER(CsrView), C.c_void_p, C.c_void_p)
+    check(L.mr_order_dbg(C.byref(A), _ptr(perm_out), _stream(stream)), "mr_order_dbg")
+
+
+def order_random(n: int, seed: int, perm_out, stream=None) -> None:
+    L = lib()
+    _sig(L.mr_order_random, C.c_int, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p)
+    check(L.mr_order_random(n, seed, _ptr(perm_out), _stream(stream)), "mr_order_random")
+
+
 GATE_SKIP, GATE_RELABEL, GATE_UNCERTAIN = 0, 1, 2
 # the trainer's scanned (tau_l, tau_h) pairs, ridge/train.py:91-99
 BAND_GATE_PAIRS = [(0.99, 1.01), (0.98, 1.02), (0.97, 1.03), (0.96, 1.04), (0.95, 1.05), (0.94, 1.06), (0.93, 1.07)]

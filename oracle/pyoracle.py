@@ -74,6 +74,7 @@ def ref():
         _sig(L.ref_hll_sampled, C.c_int, vp, i32, i32, i32, u32, i32, i32, i32, vp, vp, vp)
         _sig(L.ref_relabel_sort, C.c_int, i32, i32, vp, vp, vp, vp)
         _sig(L.ref_gorder4_full, C.c_int, i32, i32, vp, vp, vp, i32, i32, vp)
+        _sig(L.ref_relabel_order, C.c_int, i32, i32, i32, vp, vp, vp, i32, vp)
         _sig(L.ref_cusparse_spmv, C.c_int, vp, vp, vp, i32, i32, vp, vp, i32, C.POINTER(C.c_float))
         _ref = L
     return _ref
@@ -219,3 +220,31 @@ def ref_local_swap(n: int, rho: float, near: int, window: int, seed: int) -> np.
     p = np.arange(n, dtype=np.int32)
     ref().ref_local_swap(n, rho, near, window, seed, _p(p))
     return p
+
+
+# ------------------------------------------------ comparator producers ----
+
+def order_degree(rowptr, colidx):
+    """GRAPH::relabel_degree (src/class.cu:1493-1549): degree of v = count
+    of v in the column indices (desc_kernel1 over row_ind, :473-481);
+    decreasing degree, ties by increasing id (stable radix sort_by_key);
+    perm[seq[k]] = k."""
+    n = len(rowptr) - 1
+    deg = np.bincount(np.asarray(colidx, np.int64), minlength=n)[:n]
+    order = np.lexsort((np.arange(n), -deg))
+    perm = np.empty(n, np.int32)
+    perm[order] = np.arange(n, dtype=np.int32)
+    return perm
+
+
+def order_dbg(rowptr, colidx):
+    """GRAPH::dbg (src/class.cu:1660-1760): class ceilf(log2(deg + 1.0))
+    computed in double then rounded to float (dbg_kernel, :1682-1690),
+    decreasing class, increasing id (DegIdCompare, :1673-1679)."""
+    n = len(rowptr) - 1
+    deg = np.bincount(np.asarray(colidx, np.int64), minlength=n)[:n]
+    cls = np.ceil(np.log2(deg.astype(np.float64) + 1.0).astype(np.float32)).astype(np.int64)
+    order = np.lexsort((np.arange(n), -cls))
+    perm = np.empty(n, np.int32)
+    perm[order] = np.arange(n, dtype=np.int32)
+    return perm

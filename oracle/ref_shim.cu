@@ -10,7 +10,7 @@
  * Host-only entry points (run in any container): ref_get_width,
  * ref_rd_hist_exact, ref_pgorder_host, ref_predict.
  * Device entry points (need a GPU): ref_tile_build, ref_merbit_spmv,
- * ref_hll_sampled, ref_relabel_sort, ref_gorder4_full, ref_cusparse_spmv.
+ * ref_hll_sampled, ref_relabel_sort, ref_gorder4_full, ref_relabel_order, ref_cusparse_spmv.
  *
  * Index convention: the reference's `col_ind` is our row and its `row_ind`
  * is our column (src/class.cu:445-454, :1342, :1372).
@@ -183,6 +183,41 @@ int ref_gorder4_full(int nrow, int nnz, int* d_row_ind, int* d_col_ind, float* d
     g.values = d_vals;
     cudaMalloc((void**)&g.perm, sizeof(int) * nrow);
     g.gorder4(env, vsize, width);
+    cudaMemcpy(h_perm_out, g.perm, sizeof(int) * nrow, cudaMemcpyDeviceToHost);
+    cudaFree(g.perm);
+    g.perm = nullptr;
+    g.row_ind = nullptr;
+    g.col_ind = nullptr;
+    g.values = nullptr;
+    return (int)cudaDeviceSynchronize();
+}
+
+/* GRAPH::relabel_degree (kind 0, src/class.cu:1493-1549), GRAPH::dbg (kind 1,
+ * :1660-1760) or GRAPH::relabel_random (kind 2, :1460-1491) on COO arrays
+ * (row_ind = our column indices, col_ind = our row indices); perm starts as
+ * the identity, as GRAPH's constructors leave it. The COO arrays are
+ * relabelled in place by the reference. h_perm_out[old] = new. */
+int ref_relabel_order(int kind, int nrow, int nnz, int* d_row_ind, int* d_col_ind, float* d_vals, int graph_id,
+                      int* h_perm_out)
+{
+    ENV env(0, "", "");
+    cudaSetDevice(0);  // see ref_gorder4_full
+    cudaGetLastError();
+    GRAPH<float> g;
+    g.nrow = nrow;
+    g.nnz = nnz;
+    g.graph_id = graph_id;
+    g.row_ind = d_row_ind;
+    g.col_ind = d_col_ind;
+    g.values = d_vals;
+    cudaMalloc((void**)&g.perm, sizeof(int) * nrow);
+    thrust::sequence(thrust::device_ptr<int>(g.perm), thrust::device_ptr<int>(g.perm) + nrow);
+    if (kind == 0)
+        g.relabel_degree();
+    else if (kind == 1)
+        g.dbg(env);
+    else
+        g.relabel_random();
     cudaMemcpy(h_perm_out, g.perm, sizeof(int) * nrow, cudaMemcpyDeviceToHost);
     cudaFree(g.perm);
     g.perm = nullptr;
