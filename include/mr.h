@@ -230,6 +230,10 @@ typedef struct mr_server_stats {
     double mean_batch;
     double p50_us, p99_us, mean_us, max_us; /* latency: submit -> result in y */
     double req_per_s;                       /* completed / (last completion - first submit) */
+    /* per-stage time summed over batches (ms): device time of each batch's
+     * H2D copies (from its first copy, waiting included), its kernels, its
+     * D2H copies; host time the scheduler spent issuing batches */
+    double h2d_ms, compute_ms, d2h_ms, launch_ms;
 } mr_server_stats;
 
 int mr_server_create(const mr_server_config* cfg, mr_server** server);

@@ -77,7 +77,9 @@ __global__ void __launch_bounds__(kBatchWarps * 32, 1)
             lo = __ldg(prefix + it);
             hi = __ldg(prefix + it + 1);
         }
-        const MerbitOperand<V, SIGMA>& m = ops[it].m;  // fields read where used (registers are scarce)
+        // fields read where used (registers are scarce; staging the operand in
+        // shared memory measured the same)
+        const MerbitOperand<V, SIGMA>& m = ops[it].m;
         const int tile = (int)(g - lo);
         if (m.gather_mode == 0)  // warp-uniform: the default gather without a per-gather mode test
             merbit_tile<V, SIGMA, true, false, 0>(m, tile, s, pol);

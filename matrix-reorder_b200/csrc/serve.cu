@@ -188,6 +188,7 @@ struct DevVec {
 struct Lane {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_h2d = nullptr, ev_kern = nullptr;  // stage boundaries (timing)
     PinnedVec<float> hx, hy;
     PinnedVec<unsigned char> meta_h;  // the batch's small tables, one DMA per batch
     DevVec dx, dxp, dyp, dy, carry, meta_d;
@@ -220,6 +221,7 @@ struct mr_server {
     // stats
     std::vector<double> lat;
     int64_t submitted = 0, completed = 0, batches = 0, admissions = 0, evictions = 0, rejected = 0, batch_items = 0;
+    double t_h2d_ms = 0, t_kern_ms = 0, t_d2h_ms = 0, t_launch_ms = 0;  // summed over batches
     Clock::time_point t_first{}, t_last{};
     bool have_first = false;
     std::set<std::tuple<const void*, const void*, const void*, int32_t, int64_t>> validated;
@@ -406,12 +408,14 @@ int launch_batch(mr_server* s, Lane& L)
     }
     std::memcpy(mh + at_pprefix, L.off.data(), sizeof(long long) * ((size_t)count + 1));
     cudaStream_t st = L.st;
+    MR_CUDA_TRY(cudaEventRecord(L.ev_start, st));
     MR_CUDA_TRY(cudaMemcpyAsync(md, mh, meta_bytes, cudaMemcpyHostToDevice, st));
     for (int i = 0; i < count; ++i) {
         const Request* r = L.reqs[(size_t)i];
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
         MR_CUDA_TRY(cudaMemcpyAsync(dx + o, r->x_pinned ? r->x : L.hx.p + o, nb, cudaMemcpyHostToDevice, st));
     }
+    MR_CUDA_TRY(cudaEventRecord(L.ev_h2d, st));
     const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 4));
     const PermOp* d_pops = reinterpret_cast<const PermOp*>(md + at_pops);
     const long long* d_pprefix = reinterpret_cast<const long long*>(md + at_pprefix);
@@ -423,6 +427,7 @@ int launch_batch(mr_server* s, Lane& L)
                                 st));
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
     MR_CUDA_TRY(cudaGetLastError());
+    MR_CUDA_TRY(cudaEventRecord(L.ev_kern, st));
     for (int i = 0; i < count; ++i) {
         const Request* r = L.reqs[(size_t)i];
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
@@ -516,8 +521,11 @@ void scheduler_loop(mr_server* s)
         }
         L.busy = true;
         lk.unlock();
+        const auto tl = Clock::now();
         const int rc = launch_batch(s, L);
+        const double launch_ms = std::chrono::duration<double, std::milli>(Clock::now() - tl).count();
         lk.lock();
+        s->t_launch_ms += launch_ms;
         if (rc != MR_OK) {
             for (int id : L.mats) --s->mats[(size_t)id]->refs;
             finish_requests(s, L.reqs, rc);
@@ -543,12 +551,21 @@ void completion_loop(mr_server* s)
         Lane& L = s->lanes[(size_t)lane];
         lk.unlock();
         const cudaError_t e = cudaEventSynchronize(L.done);
+        float t_h2d = 0.f, t_kern = 0.f, t_d2h = 0.f;
+        if (e == cudaSuccess) {
+            cudaEventElapsedTime(&t_h2d, L.ev_start, L.ev_h2d);
+            cudaEventElapsedTime(&t_kern, L.ev_h2d, L.ev_kern);
+            cudaEventElapsedTime(&t_d2h, L.ev_kern, L.done);
+        }
         // results to the callers' buffers
         if (e == cudaSuccess)
             for (size_t i = 0; i < L.reqs.size(); ++i)
                 if (!L.reqs[i]->y_pinned)
                     std::memcpy(L.reqs[i]->y, L.hy.p + L.off[i], sizeof(float) * (size_t)(L.off[i + 1] - L.off[i]));
         lk.lock();
+        s->t_h2d_ms += t_h2d;
+        s->t_kern_ms += t_kern;
+        s->t_d2h_ms += t_d2h;
         s->inflight.pop_front();
         for (int id : L.mats) --s->mats[(size_t)id]->refs;
         finish_requests(s, L.reqs, e == cudaSuccess ? MR_OK : MR_ERR_CUDA);
@@ -591,7 +608,8 @@ int mr_server_create(const mr_server_config* cfg, mr_server** out)
               cudaMemset(s->d_flag, 0, sizeof(int)) == cudaSuccess;
     for (auto& L : s->lanes)
         ok = ok && cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) == cudaSuccess;
+             cudaEventCreate(&L.done) == cudaSuccess && cudaEventCreate(&L.ev_start) == cudaSuccess &&
+             cudaEventCreate(&L.ev_h2d) == cudaSuccess && cudaEventCreate(&L.ev_kern) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         mr_server_destroy(s);
@@ -733,6 +751,10 @@ int mr_server_get_stats(mr_server* s, mr_server_stats* out)
     for (const auto& m : s->mats) nres += m->resident ? 1 : 0;
     st.resident_matrices = nres;
     st.mean_batch = s->batches ? (double)s->batch_items / (double)s->batches : 0.0;
+    st.h2d_ms = s->t_h2d_ms;
+    st.compute_ms = s->t_kern_ms;
+    st.d2h_ms = s->t_d2h_ms;
+    st.launch_ms = s->t_launch_ms;
     if (!s->lat.empty()) {
         std::vector<double> v = s->lat;
         auto pct = [&](double q) {
@@ -763,6 +785,7 @@ int mr_server_reset_stats(mr_server* s)
     s->lat.clear();
     s->submitted -= s->completed + s->rejected;
     s->completed = s->rejected = s->batches = s->batch_items = 0;
+    s->t_h2d_ms = s->t_kern_ms = s->t_d2h_ms = s->t_launch_ms = 0;
     s->admissions = s->evictions = 0;
     s->have_first = false;
     return MR_OK;
@@ -786,7 +809,8 @@ int mr_server_destroy(mr_server* s)
     for (auto& L : s->lanes) {
         for (DevVec* d : {&L.dx, &L.dxp, &L.dyp, &L.dy, &L.carry, &L.meta_d})
             if (d->p) cudaFreeAsync(d->p, s->admit_st);
-        if (L.done) cudaEventDestroy(L.done);
+        for (cudaEvent_t ev : {L.done, L.ev_start, L.ev_h2d, L.ev_kern})
+            if (ev) cudaEventDestroy(ev);
         if (L.st) cudaStreamDestroy(L.st);
     }
     if (s->admit_st) {

@@ -628,7 +628,8 @@ class ServerStats(C.Structure):
                 ("batches", C.c_int64), ("admissions", C.c_int64), ("evictions", C.c_int64),
                 ("resident_bytes", C.c_int64), ("resident_matrices", C.c_int64), ("mean_batch", C.c_double),
                 ("p50_us", C.c_double), ("p99_us", C.c_double), ("mean_us", C.c_double), ("max_us", C.c_double),
-                ("req_per_s", C.c_double)]
+                ("req_per_s", C.c_double), ("h2d_ms", C.c_double), ("compute_ms", C.c_double), ("d2h_ms", C.c_double),
+                ("launch_ms", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
