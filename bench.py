@@ -298,6 +298,12 @@ def run_ours(args):
         yd = torch.empty_like(x_d)
         details["csr_orig_gbs"] = round(bytes_step / timed(lambda: M.spmv_csr(A, x_d, yd), 50, 5) / 1e6, 1)
         details["csr_reordered_gbs"] = round(bytes_step / timed(lambda: M.spmv_csr(B, xp, yp), 50, 5) / 1e6, 1)
+        # the reference's plain-CSR path is cuSPARSE SpMV (CSR_ALG1); torch's
+        # sparse CSR matvec calls cuSPARSE on the same arrays (library
+        # comparator, not part of this path)
+        for name, (r_, c_, v_, xx) in (("orig", (rp_d, ci_d, v_d, x_d)), ("reordered", (brp, bci, bv, xp))):
+            At = torch.sparse_csr_tensor(r_, c_, v_, size=(n, n))
+            details[f"cusparse_{name}_gbs"] = round(bytes_step / timed(lambda: torch.mv(At, xx), 50, 5) / 1e6, 1)
         plan_a = M.MerbitPlan(A, sigma=args.sigma, block=args.block)
         details["merbit_orig_gbs"] = round(bytes_step / timed(lambda: plan_a.spmv(x_d, yd), 50, 5) / 1e6, 1)
         plan_a.close()

@@ -54,6 +54,13 @@ def _edge_cases():
         "rows_fill_block": csr_from_dense_pattern([[j for j in range(3583)] for _ in range(6)]),
         "random_small": csr_random(3000, 40, seed=1, empty_frac=0.2),
         "random_wide": csr_random(2000, 300, seed=2, ncols=5000, empty_frac=0.5),
+        # row lengths around the plain CSR kernel's 2048-nonzero slices and
+        # its 4096 long-row cut, long rows back to back, empty rows between
+        # them, and trailing empty rows after a nonzero count that is a
+        # multiple of the slice
+        "slice_edges": csr_from_dense_pattern(
+            [list(range(L)) for L in (2048, 0, 0, 4096, 4097, 1, 2047, 2049, 0, 4097, 4097, 12000, 3, 0)]),
+        "slice_multiple": csr_from_dense_pattern([list(range(1024)) for _ in range(4)] + [[] for _ in range(100)]),
     }
     return cases
 
@@ -243,6 +250,22 @@ def test_csr_spmv_matches_fp64(M, O, cases, tdt):
         torch.cuda.synchronize()
         vr = vals.float().cpu().numpy()
         assert _rel_l2(y.cpu().numpy(), O.spmv_f64(rp, ci, vr, x)) <= REL_L2_F32, (name, tdt)
+
+
+def test_csr_spmv_is_deterministic(M, cases):
+    import torch
+    for name in ("huge_row", "slice_edges", "rmat13"):
+        rp, ci, v = cases[name]
+        ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+        A = M.view(_dev(rp), _dev(ci), _dev(v), n_cols=ncols)
+        x = _dev(M.uniform(ncols, seed=5))
+        ys = []
+        for _ in range(3):
+            y = torch.empty(rp.size - 1, device="cuda")
+            M.spmv_csr(A, x, y)
+            ys.append(y)
+        torch.cuda.synchronize()
+        assert all(torch.equal(ys[0].view(torch.int32), t.view(torch.int32)) for t in ys[1:]), name
 
 
 def test_plan_rejects_mismatched_matrix(M, cases):
