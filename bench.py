@@ -274,6 +274,19 @@ def run_ours(args):
     else:
         flags = 0
     hub_cache = (flags & M.PLAN_NO_HUB_CACHE) == 0
+    # pGOrder on the GPU (same permutation as the host ordering above)
+    try:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g_perm = M.pgorder_gpu(A, 0, 5)
+        torch.cuda.synchronize()
+        setup["pgorder_gpu_s"] = round(time.perf_counter() - t0, 3)
+        n2o_ref = np.empty(n, np.int32)
+        n2o_ref[perm] = np.arange(n, dtype=np.int32)
+        setup["pgorder_gpu_equals_host"] = bool(np.array_equal(g_perm.cpu().numpy(), n2o_ref))
+        del g_perm
+    except M.MRError as e:
+        setup["pgorder_gpu_s"] = f"unsupported: {e}"
     t0 = time.perf_counter()
     plan = M.MerbitPlan(B, sigma=args.sigma, block=args.block, flags=flags)
     torch.cuda.synchronize()

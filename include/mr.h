@@ -404,6 +404,16 @@ int mr_order_dbg(const mr_csr_view* A, int32_t* perm_old2new_dev, void* stream);
  * as the reference's thrust::shuffle for the same seed. */
 int mr_order_random(int32_t n, uint32_t seed, int32_t* perm_old2new_dev, void* stream);
 
+/* pGOrder on the GPU: the same permutation as mr_pgorder (bit for bit), one
+ * warp per block of vsize ids with its bucket queue in shared memory; A is a
+ * square device CSR. vsize <= 0 uses mr_pgorder_width. Returns
+ * MR_ERR_UNSUPPORTED (nothing written) when vsize > 32767, when
+ * width * (sqrt(n)/4) exceeds the 16-bit key range, or when repeated
+ * entries drive a key past it; use mr_pgorder then. Synchronises `stream`.
+ * No reference counterpart (the reference orders on host threads,
+ * GRAPH::gorder4, src/class.cu:2647-2683). */
+int mr_pgorder_gpu(const mr_csr_view* A, int32_t vsize, int32_t width, uint32_t* perm_new2old_dev, void* stream);
+
 /* ------------------------------------------ GRAPH-style host object ---- */
 
 /* A square matrix resident on the device with its current permutation

@@ -31,7 +31,7 @@ CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-ffp-contract=o
              "-I" + INCLUDE, "-I" + CSRC, "-I/usr/local/cuda/include"]
 
 CU_SOURCES = ["abi.cu", "merbit.cu", "csr.cu", "permute.cu", "rd_exact.cu", "rd_hll.cu", "graph.cu",
-              "batch.cu", "serve.cu", "noalloc.cu", "probe.cu", "producers.cu"]
+              "batch.cu", "serve.cu", "noalloc.cu", "probe.cu", "producers.cu", "pgorder_gpu.cu"]
 CXX_SOURCES = ["pgorder.cpp", "predictor.cpp"]
 HEADERS = ["common.cuh", "internal.hpp", "merbit_tile.cuh"]
 

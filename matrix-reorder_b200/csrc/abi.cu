@@ -297,6 +297,14 @@ int mr_rd_hist_sampled(const int32_t* s, int32_t nnz, int32_t samples, int32_t s
                            status, pos, as_stream(stream));
 }
 
+int mr_pgorder_gpu(const mr_csr_view* A, int32_t vsize, int32_t width, uint32_t* perm, void* stream)
+{
+    MR_TRY(check_view(A, true));
+    if (!perm && A->n_rows > 0) return MR_ERR_INVALID_ARG;
+    if (width < 1) return MR_ERR_INVALID_ARG;
+    return pgorder_gpu(A->n_rows, A->rowptr, A->colidx, (int32_t)A->nnz, vsize, width, perm, as_stream(stream));
+}
+
 int mr_band_gate(double predicted, double tau_l, double tau_h, int32_t* decision)
 {
     if (!decision || !(tau_l == tau_l) || !(tau_h == tau_h)) return MR_ERR_INVALID_ARG;

@@ -4,7 +4,9 @@
 // It keeps a square matrix resident on the device in its current order plus
 // the composed permutation perm[original] = current, and offers the
 // reference's three hot-path operations:
-//   gorder4          (src/class.cu:2608-2722): host pGOrder + device relabel
+//   gorder4          (src/class.cu:2608-2722): pGOrder (on the GPU when its
+//                    queue fits, else on host threads; the same permutation)
+//                    + device relabel
 //   locality_predict (src/class.cu:1263-1326): sampled RD + ridge predictor
 //   spmv(method)     (src/class.cu:1331-1454): "csr" or "merbit" SpMV,
 //                    returning y in the original numbering as the
@@ -130,23 +132,36 @@ int mr_graph_gorder4(mr_graph* g, int32_t vsize, int32_t width, double* ms_order
     if (!g || width < 1) return MR_ERR_INVALID_ARG;
     const int32_t n = g->n;
     if (n == 0) return MR_OK;
-    // host copies of the current structure (the reference's D2H,
-    // src/class.cu:2642-2645)
-    std::vector<int32_t> hr((size_t)n + 1), hc((size_t)std::max<int64_t>(g->nnz, 1));
-    MR_CUDA_TRY(cudaMemcpyAsync(hr.data(), g->rowptr, sizeof(int32_t) * hr.size(), cudaMemcpyDeviceToHost, g->st));
-    MR_CUDA_TRY(cudaMemcpyAsync(hc.data(), g->colidx, sizeof(int32_t) * (size_t)g->nnz, cudaMemcpyDeviceToHost, g->st));
-    MR_CUDA_TRY(cudaStreamSynchronize(g->st));
+    // the ordering: on the GPU when its queue fits (the same permutation),
+    // else on host threads from host copies of the current structure (the
+    // reference's D2H, src/class.cu:2642-2645)
     auto t0 = std::chrono::steady_clock::now();
-    std::vector<uint32_t> new2old((size_t)n);
-    MR_TRY(pgorder_host(n, hr.data(), hc.data(), vsize, width, 0, new2old.data()));
-    std::vector<int32_t> old2new((size_t)n);
-    for (int32_t i = 0; i < n; ++i) old2new[new2old[(size_t)i]] = i;
+    DevBuf step, n2o_dev;
+    MR_TRY(step.alloc(sizeof(int32_t) * (size_t)n, g->st));
+    MR_TRY(n2o_dev.alloc(sizeof(uint32_t) * (size_t)n, g->st));
+    int rc = pgorder_gpu(n, g->rowptr, g->colidx, (int32_t)g->nnz, vsize, width, n2o_dev.as<uint32_t>(), g->st);
+    if (rc == MR_OK) {
+        MR_TRY(mr_perm_invert(n, reinterpret_cast<const int32_t*>(n2o_dev.p), step.as<int32_t>(), g->st));
+    } else if (rc == MR_ERR_UNSUPPORTED) {
+        std::vector<int32_t> hr((size_t)n + 1), hc((size_t)std::max<int64_t>(g->nnz, 1));
+        MR_CUDA_TRY(cudaMemcpyAsync(hr.data(), g->rowptr, sizeof(int32_t) * hr.size(), cudaMemcpyDeviceToHost, g->st));
+        MR_CUDA_TRY(
+            cudaMemcpyAsync(hc.data(), g->colidx, sizeof(int32_t) * (size_t)g->nnz, cudaMemcpyDeviceToHost, g->st));
+        MR_CUDA_TRY(cudaStreamSynchronize(g->st));
+        t0 = std::chrono::steady_clock::now();
+        std::vector<uint32_t> new2old((size_t)n);
+        MR_TRY(pgorder_host(n, hr.data(), hc.data(), vsize, width, 0, new2old.data()));
+        std::vector<int32_t> old2new((size_t)n);
+        for (int32_t i = 0; i < n; ++i) old2new[new2old[(size_t)i]] = i;
+        MR_CUDA_TRY(
+            cudaMemcpyAsync(step.p, old2new.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, g->st));
+        MR_CUDA_TRY(cudaStreamSynchronize(g->st));  // old2new is a host local
+    } else {
+        return rc;
+    }
     if (ms_order) *ms_order = ms_since(t0);
 
     t0 = std::chrono::steady_clock::now();
-    DevBuf step;
-    MR_TRY(step.alloc(sizeof(int32_t) * (size_t)n, g->st));
-    MR_CUDA_TRY(cudaMemcpyAsync(step.p, old2new.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice, g->st));
     int32_t *nr = nullptr, *nc = nullptr;
     void* nv = nullptr;
     const size_t vb = dtype_size(g->dtype);

@@ -81,6 +81,12 @@ int pgorder_host(int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_
 int32_t pgorder_width(int32_t n, int64_t nnz);
 
 // stream-ordered scratch
+// pGOrder on the device (one warp per block of ids), bit-identical to
+// pgorder_host; MR_ERR_UNSUPPORTED when the block or key range does not fit
+// its 16-bit shared-memory queue.
+int pgorder_gpu(int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_t nnz, int32_t vsize, int32_t width,
+                uint32_t* perm, cudaStream_t st);
+
 // Stable LSD radix sort of (key, value) pairs over the low `bits` bits of the
 // keys, 8 bits per pass, ping-ponging with kbuf / vbuf: on return keys / vals
 // point at the buffers that hold the sorted pairs.

@@ -335,6 +335,18 @@ def predict_reorder(stream_dev, ncols: int, graph_id: int = 0, model: int = MODE
     return sp.value, f
 
 
+def pgorder_gpu(A: CsrView, vsize: int = 0, width: int = 5, out=None, stream=None):
+    """mr_pgorder_gpu: perm_new2old on the device (torch int32 tensor);
+    raises MRError(MR_ERR_UNSUPPORTED) where the device queue does not fit."""
+    import torch
+    L = lib()
+    _sig(L.mr_pgorder_gpu, C.c_int, C.POINTER(CsrView), C.c_int32, C.c_int32, C.c_void_p, C.c_void_p)
+    if out is None:
+        out = torch.empty(A.n_rows, dtype=torch.int32, device="cuda")
+    check(L.mr_pgorder_gpu(C.byref(A), vsize, width, _ptr(out), _stream(stream)), "mr_pgorder_gpu")
+    return out
+
+
 def pgorder_width(n: int, nnz: int) -> int:
     return int(lib().mr_pgorder_width(n, nnz))
 
