@@ -244,7 +244,9 @@ int mr_server_add_matrix(mr_server* server, int32_t n, int64_t nnz, const int32_
  * request completes (mr_server_wait / mr_server_drain). Vectors in
  * page-locked host memory (cudaHostAlloc, or cudaHostRegister covering the
  * whole vector) are copied by DMA straight from / into the caller's buffer;
- * other host memory is staged through the server's pinned buffers. */
+ * other host memory is staged through the server's pinned buffers. Whether
+ * an address is page-locked is looked up once per server (a buffer that
+ * changes kind at the same address is still copied correctly). */
 int mr_server_submit(mr_server* server, int32_t id, const float* x_host, float* y_host, uint64_t* ticket);
 /* Waits up to timeout_ms (MR_ERR_TIMEOUT after); returns the request's status. */
 int mr_server_wait(mr_server* server, uint64_t ticket, int32_t timeout_ms, double* latency_us);

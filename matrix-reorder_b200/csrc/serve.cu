@@ -9,6 +9,10 @@
 //    y = P^T y'. A matrix becomes resident on first use: upload + MERBIT plan
 //    into stream-ordered device memory, admitted against an HBM budget, the
 //    least recently used idle matrices evicted first.
+//  * Streams: each lane copies on its own stream; the kernels of all batches
+//    run in launch order on one compute stream (event-joined to the lanes),
+//    so copies of some batches overlap the kernels of others while the
+//    persistent batch kernels never contend with each other for the SMs.
 //  * Batching: a scheduler thread waits `window_us` after the first pending
 //    request (or until max_batch are pending), takes the pending requests in
 //    arrival order, admits their matrices and launches the batch on a free
@@ -216,6 +220,7 @@ struct mr_server {
     bool stop = false;
     std::thread sched, compl_;
     cudaStream_t admit_st = nullptr;
+    cudaStream_t compute_st = nullptr;  // the batches' kernels, in launch order (copies stay on the lanes)
     int* d_flag = nullptr;  // device word for launch_perm_invert
     int device = 0;
     // stats
@@ -225,6 +230,12 @@ struct mr_server {
     Clock::time_point t_first{}, t_last{};
     bool have_first = false;
     std::set<std::tuple<const void*, const void*, const void*, int32_t, int64_t>> validated;
+    // page-locked or not, per host address: the driver query once per
+    // address (a burst of submits would otherwise contend with the
+    // scheduler's copies and launches for the driver). A stale answer only
+    // changes how a vector is copied, not the result.
+    std::mutex pin_mu;
+    std::unordered_map<const void*, bool> pin_cache;
 };
 
 namespace {
@@ -416,6 +427,11 @@ int launch_batch(mr_server* s, Lane& L)
         MR_CUDA_TRY(cudaMemcpyAsync(dx + o, r->x_pinned ? r->x : L.hx.p + o, nb, cudaMemcpyHostToDevice, st));
     }
     MR_CUDA_TRY(cudaEventRecord(L.ev_h2d, st));
+    // kernels of every lane run in launch order on one stream: concurrent
+    // persistent batch kernels of several lanes only contend for the SMs
+    cudaStream_t lane_st = st;
+    st = s->compute_st;
+    MR_CUDA_TRY(cudaStreamWaitEvent(st, L.ev_h2d, 0));
     const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 4));
     const PermOp* d_pops = reinterpret_cast<const PermOp*>(md + at_pops);
     const long long* d_pprefix = reinterpret_cast<const long long*>(md + at_pprefix);
@@ -428,6 +444,8 @@ int launch_batch(mr_server* s, Lane& L)
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
     MR_CUDA_TRY(cudaGetLastError());
     MR_CUDA_TRY(cudaEventRecord(L.ev_kern, st));
+    st = lane_st;
+    MR_CUDA_TRY(cudaStreamWaitEvent(st, L.ev_kern, 0));
     for (int i = 0; i < count; ++i) {
         const Request* r = L.reqs[(size_t)i];
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
@@ -579,6 +597,24 @@ void completion_loop(mr_server* s)
 
 }  // namespace
 
+namespace {
+
+bool pinned_cached(mr_server* s, const void* p)
+{
+    {
+        std::lock_guard<std::mutex> lk(s->pin_mu);
+        auto it = s->pin_cache.find(p);
+        if (it != s->pin_cache.end()) return it->second;
+    }
+    const bool v = host_pinned(p);
+    std::lock_guard<std::mutex> lk(s->pin_mu);
+    if (s->pin_cache.size() >= 65536) s->pin_cache.clear();
+    s->pin_cache[p] = v;
+    return v;
+}
+
+}  // namespace
+
 extern "C" {
 
 int mr_server_create(const mr_server_config* cfg, mr_server** out)
@@ -604,6 +640,7 @@ int mr_server_create(const mr_server_config* cfg, mr_server** out)
     }
     s->lanes.resize((size_t)s->cfg.lanes);
     bool ok = cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->compute_st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&s->d_flag, sizeof(int)) == cudaSuccess &&
               cudaMemset(s->d_flag, 0, sizeof(int)) == cudaSuccess;
     for (auto& L : s->lanes)
@@ -676,8 +713,8 @@ int mr_server_submit(mr_server* s, int32_t id, const float* x, float* y, uint64_
     r->id = id;
     r->x = x;
     r->y = y;
-    r->x_pinned = host_pinned(x);
-    r->y_pinned = host_pinned(y);
+    r->x_pinned = pinned_cached(s, x);
+    r->y_pinned = pinned_cached(s, y);
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -818,6 +855,7 @@ int mr_server_destroy(mr_server* s)
         cudaStreamDestroy(s->admit_st);
     }
     if (s->d_flag) cudaFree(s->d_flag);
+    if (s->compute_st) cudaStreamDestroy(s->compute_st);
     for (auto& kv : s->reqs) delete kv.second;
     for (Request* r : s->pending)
         if (s->reqs.find(r->ticket) == s->reqs.end()) delete r;
