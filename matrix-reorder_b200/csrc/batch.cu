@@ -152,16 +152,16 @@ int launch_group_t(const Group& g, cudaStream_t st)
     if (g.total_tiles == 0) return MR_OK;
     const auto* ops = reinterpret_cast<const BatchOp<V, SIGMA>*>(g.ops);
     const size_t smem = sizeof(float) * (size_t)kBatchWarps * tile_smem_words<SIGMA>();
-    static std::once_flag once;
-    static cudaError_t cfg = cudaSuccess;
-    std::call_once(once, [&] {
-        cfg = cudaFuncSetAttribute(batch_spmv_kernel<V, SIGMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static PerDeviceOnce once;
+    MR_CUDA_TRY(once.run([&] {
+        cudaError_t e =
+            cudaFuncSetAttribute(batch_spmv_kernel<V, SIGMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         // smallest shared-memory carve-out that fits: the rest stays L1 for x
-        if (cfg == cudaSuccess)
-            cfg = cudaFuncSetAttribute(batch_spmv_kernel<V, SIGMA>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                       std::min(100, (int)((smem + 1023) / 1024 * 100 / 228) + 1));
-    });
-    MR_CUDA_TRY(cfg);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(batch_spmv_kernel<V, SIGMA>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     std::min(100, (int)((smem + 1023) / 1024 * 100 / 228) + 1));
+        return e;
+    }));
     batch_spmv_kernel<V, SIGMA><<<g.grid, kBatchWarps * 32, smem, st>>>(ops, g.prefix, (int)g.items.size(),
                                                                        g.total_tiles);
     MR_CUDA_TRY(cudaGetLastError());

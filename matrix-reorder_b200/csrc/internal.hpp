@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "mr.h"
 
@@ -92,6 +93,28 @@ int pgorder_gpu(int32_t n, const int32_t* rowptr, const int32_t* colidx, int32_t
 // point at the buffers that hold the sorted pairs.
 int radix_sort_pairs_u32(uint32_t*& keys, int32_t*& vals, uint32_t* kbuf, int32_t* vbuf, int64_t n, int bits,
                          cudaStream_t st);
+
+// Runs a set-up step (kernel attributes and the like) once per device: the
+// first call on each device runs it with that device current and keeps its
+// status; later calls on the device return the kept status.
+struct PerDeviceOnce {
+    std::mutex mu;
+    uint64_t done = 0;
+    cudaError_t status[64] = {};
+    template <typename F> cudaError_t run(F&& f)
+    {
+        int dev = 0;
+        const cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64) return f();  // beyond the table: every call
+        std::lock_guard<std::mutex> lk(mu);
+        if (!((done >> dev) & 1u)) {
+            status[dev] = f();
+            done |= 1ull << dev;
+        }
+        return status[dev];
+    }
+};
 
 // Stream-ordered pool of the current device for temporaries (DevBuf). It
 // keeps freed memory for reuse instead of returning it at every

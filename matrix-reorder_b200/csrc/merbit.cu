@@ -326,21 +326,20 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
     const int grid = std::max(1, std::min(sm_count(), (p.tile_num + kPersistWarps - 1) / kPersistWarps));
     if (p.hub_k > 0) {
         const size_t smem = stage + sizeof(float) * (size_t)p.hub_k;
-        static std::once_flag once;
-        static cudaError_t cfg = cudaSuccess;
-        std::call_once(once, [&] {
+        static PerDeviceOnce once;
+        MR_CUDA_TRY(once.run([&] {
             int optin = 0, dev = 0;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
             cudaFuncAttributes fa;
-            cfg = cudaFuncGetAttributes(&fa, merbit_persistent_kernel<V, SIGMA, true, GM>);
+            cudaError_t e = cudaFuncGetAttributes(&fa, merbit_persistent_kernel<V, SIGMA, true, GM>);
             // static and dynamic shared memory together may not exceed the opt-in limit
-            if (cfg == cudaSuccess)
-                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true, GM>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           optin - (int)fa.sharedSizeBytes);
-        });
-        MR_CUDA_TRY(cfg);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true, GM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         optin - (int)fa.sharedSizeBytes);
+            return e;
+        }));
         // carve-out sized to this plan's shared memory: the rest stays L1
         const int pct = std::min(100, (int)((smem + 1023) / 1024 * 100 / 228) + 1);
         MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true, GM>,
@@ -348,19 +347,18 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
         merbit_persistent_kernel<V, SIGMA, true, GM><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows,
                                                                                         p.ticket, p.hub_cols, p.hub_k);
     } else {
-        static std::once_flag once;
-        static cudaError_t cfg = cudaSuccess;
-        std::call_once(once, [&] {
-            cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false, GM>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
+        static PerDeviceOnce once;
+        MR_CUDA_TRY(once.run([&] {
+            cudaError_t e = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false, GM>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage);
             // smallest shared-memory carve-out that fits: the rest of the
             // SM's 256 KB stays L1 for x
             const int pct = (int)((stage + 1023) / 1024 * 100 / 228) + 1;
-            if (cfg == cudaSuccess)
-                cfg = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false, GM>,
-                                           cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100));
-        });
-        MR_CUDA_TRY(cfg);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, false, GM>,
+                                         cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100));
+            return e;
+        }));
         merbit_persistent_kernel<V, SIGMA, false, GM><<<grid, kPersistWarps * 32, stage, st>>>(m, p.tile_num, p.n_rows,
                                                                                           p.ticket, nullptr, 0);
     }

@@ -162,4 +162,9 @@ def test_loadgen_poisson(M, pool):
     srv.loadgen(ids, xs, ys, n_requests=2000, rate=5000.0, seed=3)
     st = srv.stats()
     assert st["completed"] == 2000 and st["req_per_s"] > 1000 and st["mean_batch"] >= 1
+    # stage timers of every batch: device copies and kernels, host launch work
+    assert st["h2d_ms"] > 0 and st["compute_ms"] > 0 and st["d2h_ms"] > 0 and st["launch_ms"] > 0
+    srv.reset_stats()
+    st = srv.stats()
+    assert st["h2d_ms"] == 0 and st["compute_ms"] == 0 and st["launch_ms"] == 0
     srv.close()
