@@ -616,6 +616,68 @@ def run_permute(args):
     return 0
 
 
+def run_csr(args):
+    """Plain CSR SpMV workload (mr_spmv_csr, the reference's cuSPARSE CSR_ALG1
+    path): R-MAT (scale, edge factor, seed as the headline) in its original
+    order and pGOrder-reordered, `steps` calls timed with CUDA events after
+    `warmup` untimed ones, beside torch's sparse CSR matvec (cuSPARSE) on the
+    same arrays. Bytes per SpMV 4(n+1) + 8 nnz + 4n (x) + 4n (y). The value is
+    the reordered matrix's; inputs are larger than L2 at the default scale."""
+    import torch
+    import mrb200 as M
+
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(a).to(dev)
+    rp, ci, v, x, perm, setup = build_workload(M, args.scale, args.edge_factor, args.seed, None)
+    n, nnz = rp.size - 1, ci.size
+    rp_d, ci_d, v_d, perm_d, x_d = d(rp), d(ci), d(v), d(perm), d(x)
+    A = M.view(rp_d, ci_d, v_d)
+    brp, bci, bv = torch.empty_like(rp_d), torch.empty_like(ci_d), torch.empty_like(v_d)
+    M.permute_csr(A, perm_d, brp, bci, bv)
+    B = M.view(brp, bci, bv)
+    xp = torch.empty_like(x_d)
+    M.permute_vector(perm_d, x_d, xp, inverse=False)
+    st = torch.cuda.current_stream()
+    b = spmv_bytes(n, nnz)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    out = {}
+    for name, Mv, rpx, cix, vx, xx in (("orig", A, rp_d, ci_d, v_d, x_d), ("reordered", B, brp, bci, bv, xp)):
+        y = torch.empty_like(xx)
+        ms = timed(lambda: M.spmv_csr(Mv, xx, y))
+        S = torch.sparse_csr_tensor(rpx, cix, vx, size=(n, n))
+        ms_c = timed(lambda: torch.mv(S, xx))
+        ref = torch.mv(S.double(), xx.double())
+        rel = float((y.double() - ref).norm() / ref.norm())
+        out[name] = {"ms": round(ms, 4), "gbs": round(b / ms / 1e6, 1), "cusparse_gbs": round(b / ms_c / 1e6, 1),
+                     "rel_l2_vs_fp64": rel}
+        del S, ref
+    peak, peak_kind = peaks()
+    gbs = out["reordered"]["gbs"]
+    line = {"metric": "csr_spmv_gbs", "value": gbs, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["reordered"]["ms"], "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"rmat_s{args.scale}_ef{args.edge_factor} plain CSR SpMV, pGOrder-reordered",
+                       "n_rows": n, "nnz": nnz, "l2": "inputs larger than L2 at scale >= 21"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": round(gbs / peak, 4),
+                         "peak_kind": peak_kind, "algorithmic_bytes": b,
+                         "kernels_timed": "csr_stream_kernel + csr_long_rows_kernel"},
+            "details": dict(out, **setup)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_serve(args):
     """Serving workload: a resident pool of pGOrder-reordered FP16 matrices
     (rows log-uniform 4K..2M, degree 4..64, R-MAT / banded / Chung-Lu),
@@ -907,7 +969,7 @@ def main() -> int:
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of CPU-baseline timing")
     ap.add_argument("--quick", action="store_true", help="skip companion numbers and CPU baseline")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="use --sigma/--block instead of the autotuner")
-    ap.add_argument("--workload", choices=["spmv", "serve", "precision", "batch", "permute"], default="spmv")
+    ap.add_argument("--workload", choices=["spmv", "serve", "precision", "batch", "permute", "csr"], default="spmv")
     ap.add_argument("--cl-rows", type=int, default=8 * 1024 * 1024, help="precision: Chung-Lu rows")
     ap.add_argument("--pool", type=int, default=2000, help="serve: resident matrices")
     ap.add_argument("--protos", type=int, default=24, help="serve: distinct generated matrices in the pool")
@@ -931,6 +993,8 @@ def main() -> int:
         return run_precision(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "csr":
+        return run_csr(args)
     if args.workload == "permute":
         return run_permute(args)
     return run_ours(args)

@@ -1,21 +1,21 @@
 // Plain CSR SpMV for sm_100a (the reference's cuSPARSE CSR_ALG1 path,
 // src/class.cu:1359-1397, replaced by a hand-written kernel).
 //
-// Two kernels, both deterministic (every row is summed by one lane group or
-// one CTA, in a fixed order):
-//  * csr_vector_kernel: groups of G lanes (G = 2..32, picked from the mean
-//    row length), one row per group at a time; lanes stride the row with
-//    evict-first loads of colidx and values, gather x through L2 with an
-//    evict-last policy, and reduce with a fixed shuffle tree. Every warp owns
-//    a contiguous chunk of rows and its groups take adjacent rows of the
-//    chunk, so the loads of a warp stay coalesced and a heavy row lands in
-//    its own warp: a plain grid-stride over rows would hand the rows that are
-//    equal modulo the stride to the same group, and orders that start every
-//    block of ids with its heaviest vertex (pGOrder partitions of 1024)
-//    would then pile the heavy rows onto a few groups. With narrow groups
-//    (MED), rows of more than kMedRow nonzeros are deferred to a per-warp
-//    list in shared memory and summed afterwards by the whole warp; rows
-//    longer than kLongRow are skipped and appended to a global list.
+// Two kernels, both deterministic (every sum is formed in a fixed order that
+// does not depend on timing):
+//  * csr_stream_kernel: every warp owns the rows between two merge-path
+//    diagonals of (rows, nonzeros), an equal share of both, found by a
+//    warp-wide 33-ary search of i + rowptr[i]. Its nonzeros are streamed in
+//    tiles of 128, four consecutive nonzeros per lane (16-byte evict-first
+//    loads of colidx and values, x gathered through L2 with an evict-last
+//    policy); the next tile's loads are issued before the current tile is
+//    summed. Each lane finds the row of its first nonzero by a shuffle
+//    search over the next 32 row starts, sums its nonzeros row by row and
+//    writes the rows that lie inside it; the parts of rows that cross lanes
+//    are joined by one segmented warp scan and written by the lane holding
+//    the row's last nonzero, and the row open at the tile end is carried to
+//    the next tile. Empty rows are zeroed; rows longer than kLongRow are
+//    skipped and appended to a global list.
 //  * csr_long_rows_kernel: one 1024-thread CTA per listed row, a fixed
 //    per-thread stride (four loads in flight) and a fixed shared-memory tree.
 #include <atomic>
@@ -28,76 +28,9 @@ namespace mr {
 
 constexpr int kLongRow = 4096;
 constexpr int kLongThreads = 1024;
-constexpr int kMedRow = 32;     // narrow groups defer longer rows to the whole warp
-constexpr int kMedList = 256;   // deferral only for warps whose chunk has at most this many rows
-
-template <typename V, int G, bool MED>
-__global__ void __launch_bounds__(256)
-    csr_vector_kernel(int n, const int* __restrict__ rowptr, const int* __restrict__ colidx, const V* __restrict__ vals,
-                      const float* __restrict__ x, float* __restrict__ y, int* __restrict__ long_rows,
-                      int* __restrict__ n_long)
-{
-    constexpr int GPW = 32 / G;  // groups per warp
-    __shared__ int s_med[MED ? 8 : 1][MED ? kMedList : 1];
-    __shared__ int s_nmed[8];
-    const uint64_t pol = l2_evict_last_policy();
-    const int lane = threadIdx.x & (G - 1);
-    const int gi = (threadIdx.x & 31) / G;
-    // the group's own lanes: groups of one warp run different rows, so every
-    // shuffle names only its group
-    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int chunk = ((n + warps - 1) / warps + GPW - 1) / GPW * GPW;
-    const int r0 = min(n, warp * chunk), r1 = min(n, r0 + chunk);
-    const int wl = (threadIdx.x >> 5);  // warp in the CTA
-    // deferring only when the whole chunk fits the list keeps the choice of
-    // who sums a row independent of timing
-    const bool defer = MED && (r1 - r0) <= kMedList;
-    if (MED && (threadIdx.x & 31) == 0) s_nmed[wl] = 0;
-    __syncwarp();
-    for (int row = r0 + gi; row < r1; row += GPW) {
-        const int b = __ldg(rowptr + row), e = __ldg(rowptr + row + 1);
-        if (e - b > kLongRow) {
-            if (lane == 0) long_rows[atomicAdd(n_long, 1)] = row;
-            continue;
-        }
-        if constexpr (MED) {
-            if (defer && e - b > kMedRow) {
-                if (lane == 0) s_med[wl][atomicAdd(&s_nmed[wl], 1)] = row;
-                continue;  // the warp sums it below
-            }
-        }
-        float s = 0.f;
-        for (int k = b + lane; k < e; k += G)
-            s += ValueTraits<V>::f(ld_stream(vals + k)) * ld_x(x + ld_stream(colidx + k), pol);
-#pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(gmask, s, o, G);
-        if (lane == 0) y[row] = s;
-    }
-    if constexpr (MED) {
-        // deferred rows, in list order, one warp each
-        __syncwarp();
-        const int l = threadIdx.x & 31;
-        const int cnt = s_nmed[wl];
-        for (int i = 0; i < cnt; ++i) {
-            const int row = s_med[wl][i];
-            const int b = __ldg(rowptr + row), e = __ldg(rowptr + row + 1);
-            float s = 0.f;
-            for (int k = b + l; k < e; k += 32)
-                s += ValueTraits<V>::f(ld_stream(vals + k)) * ld_x(x + ld_stream(colidx + k), pol);
-            s = warp_sum(s);
-            if (l == 0) y[row] = s;
-        }
-    }
-}
-
-#ifndef CSR_STREAM
-#define CSR_STREAM 1
-#endif
-constexpr int kQ = 4;           // consecutive nonzeros per lane in a tile
-constexpr int kTile = 32 * kQ;  // nonzeros per warp tile
-constexpr int kTiles = 2;       // tiles whose loads are issued together
+constexpr int kQ = 4;               // consecutive nonzeros per lane in a tile
+constexpr int kTileNnz = 32 * kQ;   // nonzeros per warp tile
+constexpr int kWarpsPerCta = 8;
 
 // Row of element k: the last row r in [rcur, rend) whose first nonzero is at
 // or before k (an empty row shares its start with the next row, so this is
@@ -134,42 +67,52 @@ __device__ __forceinline__ int csr_row_of(const int* __restrict__ rowptr, int rc
     return row;
 }
 
-template <typename V, bool VEC>
-__device__ __forceinline__ void csr_quad(const int* __restrict__ colidx, const V* __restrict__ vals,
-                                         const float* __restrict__ x, uint64_t pol, int k0, int ea, int eb,
-                                         float (&p)[kQ])
+// Products of the Q nonzeros k0 .. k0+Q-1 (zero outside [ea, eb)); whole
+// groups of four in range are vector loads.
+// Column indices and values of the Q nonzeros k0 .. k0+Q-1; outside
+// [ea, eb) the column is -1.
+template <typename V, bool VEC, int Q>
+__device__ __forceinline__ void csr_ld_stream(const int* __restrict__ colidx, const V* __restrict__ vals, int k0,
+                                              int ea, int eb, int (&c)[Q], float (&w)[Q])
 {
-    if (VEC && k0 >= ea && k0 + kQ <= eb) {
-        const int4 c = ld_stream(reinterpret_cast<const int4*>(colidx + k0));
-        float v[4];
-        Vec4<V>::unpack(ld_stream(reinterpret_cast<const typename Vec4<V>::T*>(vals + k0)), v);
-        p[0] = v[0] * ld_x(x + c.x, pol);
-        p[1] = v[1] * ld_x(x + c.y, pol);
-        p[2] = v[2] * ld_x(x + c.z, pol);
-        p[3] = v[3] * ld_x(x + c.w, pol);
+    if (VEC && k0 >= ea && k0 + Q <= eb) {
+#pragma unroll
+        for (int i = 0; i < Q / 4; ++i) {
+            const int4 ci = ld_stream(reinterpret_cast<const int4*>(colidx + k0) + i);
+            float v[4];
+            Vec4<V>::unpack(ld_stream(reinterpret_cast<const typename Vec4<V>::T*>(vals + k0) + i), v);
+            c[4 * i + 0] = ci.x;
+            c[4 * i + 1] = ci.y;
+            c[4 * i + 2] = ci.z;
+            c[4 * i + 3] = ci.w;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[4 * i + j] = v[j];
+        }
     } else {
 #pragma unroll
-        for (int j = 0; j < kQ; ++j) {
+        for (int j = 0; j < Q; ++j) {
             const int k = k0 + j;
-            p[j] = k >= ea && k < eb ? ValueTraits<V>::f(ld_stream(vals + k)) * ld_x(x + ld_stream(colidx + k), pol)
-                                     : 0.f;
+            const bool in = k >= ea && k < eb;
+            c[j] = in ? ld_stream(colidx + k) : -1;
+            w[j] = in ? ValueTraits<V>::f(ld_stream(vals + k)) : 0.f;
         }
     }
 }
 
-// One tile: elements [tb, tb + kTile) of the run [ea, eb) (rows up to rb),
-// lane l holding tb + 4l .. tb + 4l + 3 with products p. Each lane sums its
+// One tile: elements [tb, tb + 32Q) of the run [ea, eb) (rows up to rb),
+// lane l holding tb + Ql .. tb + Ql + Q-1 with products p. Each lane sums its
 // elements row by row; a row wholly inside a lane is written by it; the
 // parts of rows that cross lanes are joined by one segmented warp scan and
 // written by the lane holding the row's last element; the row still open at
 // the tile end is carried (open_row, carry). rcur is a row at or before the
 // tile's first element.
+template <int Q>
 __device__ __forceinline__ void csr_tile(int tb, int ea, int eb, int rb, const int* __restrict__ rowptr,
-                                         float* __restrict__ y, const float (&p)[kQ], int lane, int& rcur,
+                                         float* __restrict__ y, const float (&p)[Q], int lane, int& rcur,
                                          int& open_row, float& carry)
 {
-    const int k0 = tb + kQ * lane;
-    const int klo = max(k0, ea), khi = min(k0 + kQ, eb) - 1;
+    const int k0 = tb + Q * lane;
+    const int klo = max(k0, ea), khi = min(k0 + Q, eb) - 1;
     const bool any = klo <= khi;
     int nxt;
     int row = csr_row_of(rowptr, rcur, rb, eb, any ? klo : (k0 < ea ? ea : eb - 1), lane, &nxt);
@@ -177,7 +120,7 @@ __device__ __forceinline__ void csr_tile(int tb, int ea, int eb, int rb, const i
     float s = 0.f, s_first = 0.f;
     bool multi = false;  // the first row ended inside the lane
 #pragma unroll
-    for (int j = 0; j < kQ; ++j) {
+    for (int j = 0; j < Q; ++j) {
         const int k = k0 + j;
         if (k >= klo && k <= khi) {
             while (k >= nxt) {  // row `row` ended before k
@@ -230,9 +173,10 @@ __device__ __forceinline__ void csr_tile(int tb, int ea, int eb, int rb, const i
     if (r31 >= 0) rcur = r31;
 }
 
-// The rows [ra, rb) of one warp, none longer than kLongRow and at least one
-// nonzero among them: tiles of kTile nonzeros from ea rounded down to a
-// multiple of 4. Fixed tiles, fixed order: deterministic.
+// The rows [ra, rb) of one warp, none longer than kLongRow, at least one
+// nonzero among them: tiles of kTileNnz nonzeros from ea rounded down to a
+// multiple of 4, the next tile's index and value loads in flight while the
+// current tile is summed. Fixed tiles, fixed order: deterministic.
 template <typename V, bool VEC>
 __device__ __forceinline__ void csr_stream_rows(int ra, int rb, const int* __restrict__ rowptr,
                                                 const int* __restrict__ colidx, const V* __restrict__ vals,
@@ -242,16 +186,15 @@ __device__ __forceinline__ void csr_stream_rows(int ra, int rb, const int* __res
     const int ea = __ldg(rowptr + ra), eb = __ldg(rowptr + rb);
     int rcur = ra, open_row = -1;
     float carry = 0.f;
-    for (int base = ea & ~(kQ - 1); base < eb; base += kTile * kTiles) {
-        float p[kTiles][kQ];
+    int c[kQ];
+    float w[kQ];
+    csr_ld_stream<V, VEC, kQ>(colidx, vals, (ea & ~3) + kQ * lane, ea, eb, c, w);
+    for (int base = ea & ~3; base < eb; base += kTileNnz) {
+        float p[kQ];
 #pragma unroll
-        for (int t = 0; t < kTiles; ++t) csr_quad<V, VEC>(colidx, vals, x, pol, base + t * kTile + kQ * lane, ea, eb, p[t]);
-#pragma unroll
-        for (int t = 0; t < kTiles; ++t) {
-            const int tb = base + t * kTile;
-            if (tb >= eb) break;
-            csr_tile(tb, ea, eb, rb, rowptr, y, p[t], lane, rcur, open_row, carry);
-        }
+        for (int j = 0; j < kQ; ++j) p[j] = c[j] >= 0 ? w[j] * ld_x(x + c[j], pol) : 0.f;
+        if (base + kTileNnz < eb) csr_ld_stream<V, VEC, kQ>(colidx, vals, base + kTileNnz + kQ * lane, ea, eb, c, w);
+        csr_tile<kQ>(base, ea, eb, rb, rowptr, y, p, lane, rcur, open_row, carry);
     }
 }
 
@@ -281,7 +224,7 @@ __device__ __forceinline__ int csr_merge_row(const int* __restrict__ rowptr, int
 // of rows + nonzeros: empty rows are zeroed, rows longer than kLongRow go to
 // the global list, the runs of other rows are streamed.
 template <typename V, bool VEC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kWarpsPerCta * 32)
     csr_stream_kernel(int n, int nnz, const int* __restrict__ rowptr, const int* __restrict__ colidx,
                       const V* __restrict__ vals, const float* __restrict__ x, float* __restrict__ y,
                       int* __restrict__ long_rows, int* __restrict__ n_long)
@@ -374,50 +317,28 @@ static int launch_t(int n, int64_t nnz, const int* rowptr, const int* colidx, co
     int* long_rows = n_long + 1;
     MR_CUDA_TRY(cudaMemsetAsync(n_long, 0, sizeof(int), st));
     const V* v = reinterpret_cast<const V*>(vals);
-#if CSR_STREAM
-    {
-        // equal merge-path shares, two per resident warp slot, at least 512
-        // rows + nonzeros per warp
-        static PerDeviceOnce occ_once;
-        static std::atomic<int> occ{0};
-        MR_CUDA_TRY(occ_once.run([&] {
-            int b = 0;
-            const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, csr_stream_kernel<V, true>, 256, 0);
-            if (e == cudaSuccess) occ.store(std::max(1, b));
-            return e;
-        }));
-        const long long total = (long long)n + nnz;
-        const long long cap = (long long)sm_count() * std::max(1, occ.load()) * 2;
-        const int grid = (int)std::max<long long>(1, std::min<long long>(cap, (total + 8 * 512 - 1) / (8 * 512)));
-        const bool vec = (reinterpret_cast<uintptr_t>(colidx) & 15) == 0 &&
-                         (reinterpret_cast<uintptr_t>(vals) & (4 * sizeof(V) - 1)) == 0;
-        if (vec)
-            csr_stream_kernel<V, true><<<grid, 256, 0, st>>>(n, (int)nnz, rowptr, colidx, v, x, y, long_rows, n_long);
-        else
-            csr_stream_kernel<V, false><<<grid, 256, 0, st>>>(n, (int)nnz, rowptr, colidx, v, x, y, long_rows, n_long);
-        MR_CUDA_TRY(cudaGetLastError());
-        if (nnz > kLongRow) {
-            const int lg = (int)std::max<int64_t>(1, std::min<int64_t>(max_long, (int64_t)sm_count() * 2));
-            csr_long_rows_kernel<V><<<lg, kLongThreads, 0, st>>>(rowptr, colidx, v, x, y, long_rows, n_long);
-            MR_CUDA_TRY(cudaGetLastError());
-        }
-        return MR_OK;
-    }
-#endif
-    // lanes per row from the mean row length; below 24 the groups stay narrow
-    // and rows above kMedRow go to the whole warp
-    const double mean = (double)nnz / (double)n;
-    const int g = mean <= 3 ? 2 : mean <= 6 ? 4 : mean <= 24 ? 8 : 32;
-    const long long want = ((long long)n * g + 255) / 256;
-    const int grid = (int)std::max<long long>(1, std::min<long long>(want, (long long)sm_count() * 32));
-    switch (g) {
-    case 2: csr_vector_kernel<V, 2, true><<<grid, 256, 0, st>>>(n, rowptr, colidx, v, x, y, long_rows, n_long); break;
-    case 4: csr_vector_kernel<V, 4, true><<<grid, 256, 0, st>>>(n, rowptr, colidx, v, x, y, long_rows, n_long); break;
-    case 8: csr_vector_kernel<V, 8, true><<<grid, 256, 0, st>>>(n, rowptr, colidx, v, x, y, long_rows, n_long); break;
-    default:
-        csr_vector_kernel<V, 32, false><<<grid, 256, 0, st>>>(n, rowptr, colidx, v, x, y, long_rows, n_long);
-        break;
-    }
+    const long long total = (long long)n + nnz;
+    // two merge-path shares per resident warp, at least 512 rows + nonzeros each
+    static PerDeviceOnce occ_once;
+    static std::atomic<int> occ{0};
+    MR_CUDA_TRY(occ_once.run([&] {
+        int b = 0;
+        const cudaError_t e =
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, csr_stream_kernel<V, true>, kWarpsPerCta * 32, 0);
+        if (e == cudaSuccess) occ.store(std::max(1, b));
+        return e;
+    }));
+    const long long cap = (long long)sm_count() * std::max(1, occ.load()) * 2;
+    const long long per_cta = (long long)kWarpsPerCta * 512;
+    const int grid = (int)std::max<long long>(1, std::min<long long>(cap, (total + per_cta - 1) / per_cta));
+    const bool vec = (reinterpret_cast<uintptr_t>(colidx) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(vals) & (4 * sizeof(V) - 1)) == 0;
+    if (vec)
+        csr_stream_kernel<V, true><<<grid, kWarpsPerCta * 32, 0, st>>>(n, (int)nnz, rowptr, colidx, v, x, y,
+                                                                      long_rows, n_long);
+    else
+        csr_stream_kernel<V, false><<<grid, kWarpsPerCta * 32, 0, st>>>(n, (int)nnz, rowptr, colidx, v, x, y,
+                                                                       long_rows, n_long);
     MR_CUDA_TRY(cudaGetLastError());
     if (nnz > kLongRow) {
         const int lg = (int)std::max<int64_t>(1, std::min<int64_t>(max_long, (int64_t)sm_count() * 2));
