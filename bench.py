@@ -402,7 +402,7 @@ def run_ours(args):
     # requests overlap across lanes (copies of one with the SpMV of others).
     # Time = first submit to last result, from the server's own clock.
     brp_h, bci_h, bv_h = brp.cpu().numpy(), bci.cpu().numpy(), bv.cpu().numpy()
-    srv = M.Server(window_us=50, max_batch=4, lanes=4, sigma=args.sigma)
+    srv = M.Server(window_us=20, max_batch=2, lanes=8, sigma=args.sigma)
     sid = srv.add_matrix(brp_h, bci_h, bv_h, perm)
     y_ring = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(8)]
     y_ring_np = [t.numpy() for t in y_ring]
@@ -423,6 +423,9 @@ def run_ours(args):
         tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
         ms_served = float(t.item())
     e2e_val = ws * bytes_step * k_e2e / (ms_served / 1e3) / 1e9
+    # the copy ceiling of one step: x host->device and y device->host of the
+    # same sizes, concurrently on two streams, nothing else
+    pcie = pcie_ceiling(torch, dev, n)
     served_check = float(torch.linalg.norm(y_ring[(k_e2e - 1) % 8].to(dev).double() - y_h.to(dev).double()) /
                          torch.linalg.norm(y_h.to(dev).double()))
     # self-check of the e2e result: against the plain CSR kernel on the
@@ -475,8 +478,9 @@ def run_ours(args):
             "roofline": roofline,
             "e2e": {"value": round(e2e_val, 1), "unit": "GB/s", "h2d_bytes_per_step": 4 * n,
                     "d2h_bytes_per_step": 4 * n, "steps": k_e2e, "ms_per_step": round(ms_served / k_e2e, 4),
-                    "path": "mr_server (C-ABI request API, pinned host x/y, requests overlapped on 4 lanes, "
+                    "path": "mr_server (C-ABI request API, pinned host x/y, requests overlapped on 8 lanes, "
                             "batched MERBIT without hub cache)",
+                    "copy_ceiling": dict(pcie, frac=round(pcie["bidir_ms_per_step"] / (ms_served / k_e2e), 4)),
                     "served_vs_sync_rel_l2": served_check,
                     "sync": {"value": round(e2e_sync_val, 1), "ms_per_step": round(ms_e2e / k_e2e, 4),
                              "path": "mr_plain_requests (C-ABI, pinned host x/y, synchronised per step)",
@@ -614,6 +618,37 @@ def run_permute(args):
             "details": setup}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def pcie_ceiling(torch, dev, n, reps=100, trials=3):
+    """Host<->device copy ceiling of one e2e step: n floats host->device and n
+    floats device->host from/to page-locked memory, alone and concurrently on
+    two streams; host clock around `reps` copies after a synchronise, best of
+    `trials` (a step is both directions)."""
+    hb = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(2)]
+    db = [torch.empty(n, dtype=torch.float32, device=dev) for _ in range(2)]
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def run(h2d, d2h):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            if h2d:
+                with torch.cuda.stream(s1):
+                    db[0].copy_(hb[0], non_blocking=True)
+            if d2h:
+                with torch.cuda.stream(s2):
+                    hb[1].copy_(db[1], non_blocking=True)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / reps
+
+    run(True, True)
+    ms_h = min(run(True, False) for _ in range(trials))
+    ms_d = min(run(False, True) for _ in range(trials))
+    ms_b = min(run(True, True) for _ in range(trials))
+    b = 4 * n
+    return {"h2d_gbs": round(b / ms_h / 1e6, 1), "d2h_gbs": round(b / ms_d / 1e6, 1),
+            "bidir_ms_per_step": round(ms_b, 4), "bidir_gbs_per_direction": round(b / ms_b / 1e6, 1)}
 
 
 def run_csr(args):

@@ -149,6 +149,7 @@ int mr_merbit_plan_create_ex(const mr_csr_view* A, int sigma, int block, int fla
         cudaFree(p.ticket);
         cudaFree(p.colh);
         cudaFree(p.hub_cols);
+        cudaFree(p.chunk_start);
         delete h;
         return code;
     };
@@ -171,6 +172,10 @@ int mr_merbit_plan_create_ex(const mr_csr_view* A, int sigma, int block, int fla
         s = build_hub_cache(p, *A, st);
         if (s != MR_OK) return fail(s);
     }
+    if (block == 1024) {
+        s = build_chunk_bounds(p, A->colidx, st);
+        if (s != MR_OK) return fail(s);
+    }
     *out = h;
     return MR_OK;
 }
@@ -189,6 +194,7 @@ int mr_merbit_plan_destroy(mr_merbit_plan* h)
     cudaFree(h->p.ticket);
     cudaFree(h->p.colh);
     cudaFree(h->p.hub_cols);
+    cudaFree(h->p.chunk_start);
     if (dev != h->p.device) cudaSetDevice(dev);
     delete h;
     return MR_OK;

@@ -34,6 +34,10 @@ struct MerbitPlan {
     int hub_limit = 0;            // cap on hub slots (0: as many as fit)
     int gather_mode = 0;          // x gather cache path (ld_x_mode)
     int device = 0;
+    // persistent kernel: tile chunk of each CTA, chunk_start[c] .. chunk_start[c+1],
+    // balanced by estimated cost (chunks + 1 entries); nullptr: equal tile counts
+    int32_t* chunk_start = nullptr;
+    int chunks = 0;
 };
 
 int launch_merbit_plan(const int* rowptr, int nrow, int nnz, int sigma, int lane_num, int tile_num, uint32_t* tile_x,
@@ -43,6 +47,10 @@ int launch_merbit_spmv(const MerbitPlan& p, const int* colidx, const void* vals,
 bool merbit_sigma_supported(int sigma);
 // builds the hub cache of a persistent-kernel plan (no-op when it would not pay)
 int build_hub_cache(MerbitPlan& p, const mr_csr_view& A, cudaStream_t st);
+// cost-balanced CTA chunks of a persistent-kernel plan (after the hub cache)
+int build_chunk_bounds(MerbitPlan& p, const int* colidx, cudaStream_t st);
+// CTAs of the persistent kernel for a plan of tile_num tiles on this device
+int persistent_grid(int tile_num);
 // largest number of hub slots that fit beside the SIGMA staging buffers
 int hub_capacity(int sigma);
 

@@ -156,11 +156,15 @@ __global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOpe
 
 // ---- persistent form: one CTA of 32 warps per SM sweeps a contiguous chunk
 // of tiles, so the warps resident on an SM work on neighbouring rows and the
-// reordered matrix's x reuse is caught by L1 (the streams bypass L1). Rows
-// whose carry run stays inside a chunk are finished by the chunk's CTA after
-// a barrier; the last CTA to finish (atomic ticket after a fence) finishes
-// the runs that cross chunk boundaries. Same FP64 run sums, same order, as
-// the two-kernel form: the results are bit-identical.
+// reordered matrix's x reuse is caught by L1 (the streams bypass L1). The
+// chunk bounds come from the plan, balanced by estimated cost (a tile's x
+// gathers that miss the hub cache dominate its time, so equal tile counts
+// leave some SMs working 20% longer than the mean), or are equal tile counts
+// when the plan has none. Rows whose carry run stays inside a chunk are
+// finished by the chunk's CTA after a barrier; the last CTA to finish
+// (atomic ticket after a fence) finishes the runs that cross chunk
+// boundaries. Same FP64 run sums, same order, as the two-kernel form: the
+// results are bit-identical.
 constexpr int kPersistWarps = 32;
 
 __device__ __forceinline__ int open_row(const uint32_t* tile_y, int t)
@@ -185,38 +189,65 @@ __device__ __forceinline__ void fixup_in_chunk(const uint32_t* __restrict__ tile
     y[R] = (float)((double)y[R] + acc);
 }
 
-// run that crosses the boundary at the start of chunk c and whose row ends
-// inside chunk c (each crossing run is finished at exactly one boundary)
-__device__ __forceinline__ void fixup_boundary(const uint32_t* __restrict__ tile_y, const float* carry, int tile_num,
-                                               int chunk, int nrow, float* y, int c)
+// Run that crosses the boundary b at the start of a chunk [b, e) and whose
+// row ends inside that chunk (each crossing run is finished at exactly one
+// boundary; an empty chunk finishes none), for one warp: the run's ends are
+// found 32 tiles per step with ballots (open rows never decrease along the
+// tiles, so a run is contiguous), and its carries are summed in FP64 in tile
+// order, as in fixup_in_chunk.
+__device__ __forceinline__ void fixup_boundary_warp(const uint32_t* __restrict__ tile_y, const float* carry,
+                                                    int tile_num, int b, int e, int nrow, float* y, int lane)
 {
-    const int b = c * chunk;
     if (b <= 0 || b >= tile_num) return;
     const int p = b - 1;
     const int R = open_row(tile_y, p);
     if (R >= nrow) return;
-    int ue = p;
-    while (ue + 1 < tile_num && open_row(tile_y, ue + 1) == R) ++ue;
-    if (ue + 1 >= min(b + chunk, tile_num)) return;  // ends beyond chunk c
-    int u0 = p;
-    while (u0 > 0 && open_row(tile_y, u0 - 1) == R) --u0;
+    int ue = p;  // last tile of the run
+    for (;;) {
+        const int q = ue + 1 + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, q < tile_num && open_row(tile_y, q) == R);
+        if (m != 0xffffffffu) {
+            ue += __ffs(~m) - 1;
+            break;
+        }
+        ue += 32;
+    }
+    if (ue + 1 >= e) return;  // ends beyond this chunk
+    int u0 = p;  // first tile of the run
+    for (;;) {
+        const int q = u0 - 1 - lane;
+        const unsigned m = __ballot_sync(0xffffffffu, q >= 0 && open_row(tile_y, q) == R);
+        if (m != 0xffffffffu) {
+            u0 -= __ffs(~m) - 1;
+            break;
+        }
+        u0 -= 32;
+    }
     double acc = 0.0;
-    for (int u = u0; u <= ue; ++u) acc += (double)__ldcg(carry + u);
-    y[R] = (float)((double)__ldcg(y + R) + acc);
+    for (int base = u0; base <= ue; base += 32) {
+        const float c = base + lane <= ue ? __ldcg(carry + base + lane) : 0.f;
+        const int cnt = min(32, ue - base + 1);
+        for (int j = 0; j < cnt; ++j) acc += (double)__shfl_sync(0xffffffffu, c, j);
+    }
+    if (lane == 0) y[R] = (float)((double)__ldcg(y + R) + acc);
 }
 
 template <typename V, int SIGMA, bool HUB, int GM>
 __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     merbit_persistent_kernel(const MerbitOperand<V, SIGMA> m_in, int tile_num, int nrow, int* __restrict__ ticket,
-                             const int32_t* __restrict__ hub_cols, int hub_k)
+                             const int32_t* __restrict__ hub_cols, int hub_k, const int32_t* __restrict__ chunk_start)
 {
     extern __shared__ __align__(16) float s_dyn[];
-    __shared__ int s_last;
+    __shared__ int s_last, s_nlong;
     const int warp = threadIdx.x >> 5;
     const int G = gridDim.x;
     const int chunk = (tile_num + G - 1) / G;
-    const int t0 = min((int)blockIdx.x * chunk, tile_num);
-    const int t1 = min(t0 + chunk, tile_num);
+    // chunk c = [start(c), start(c + 1))
+    auto start = [&](int c) {
+        return chunk_start ? (c >= G ? tile_num : __ldg(chunk_start + c)) : min(c * chunk, tile_num);
+    };
+    const int t0 = start(blockIdx.x);
+    const int t1 = start(blockIdx.x + 1);
     float* s = s_dyn + warp * tile_smem_words<SIGMA>();
     const TilePolicy pol{l2_evict_last_policy(), l2_evict_first_policy()};
     MerbitOperand<V, SIGMA> m = m_in;
@@ -246,14 +277,71 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     }
     for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true, HUB, GM>(m, t, s, pol);
     __syncthreads();
-    for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x) fixup_in_chunk(m.tile_y, m.carry, t0, t1, nrow, m.y, t);
+    // runs inside the chunk: open rows and carries staged in the (now free)
+    // tile staging memory, so a run is walked in shared memory rather than
+    // one dependent global load per tile
+    constexpr int kStageWords = kPersistWarps * tile_smem_words<SIGMA>();
+    const int nt = t1 - t0;
+    if (nt <= kStageWords / 2) {
+        int* sR = reinterpret_cast<int*>(s_dyn);
+        float* sC = s_dyn + kStageWords / 2;
+        for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+            sR[i] = open_row(m.tile_y, t0 + i);
+            sC[i] = m.carry[t0 + i];
+        }
+        const int r_before = t0 > 0 ? open_row(m.tile_y, t0 - 1) : -1;
+        __syncthreads();
+        for (int i = threadIdx.x; i < nt; i += blockDim.x) {
+            const int R = sR[i];
+            if (R >= nrow) continue;
+            if (t0 + i > 0 && (i > 0 ? sR[i - 1] : r_before) == R) continue;  // not the first tile of its run
+            double acc = 0.0;
+            int u = i;
+            while (u < nt && sR[u] == R) {
+                acc += (double)sC[u];
+                ++u;
+            }
+            if (u >= nt) continue;  // the row ends in a later chunk: boundary pass
+            m.y[R] = (float)((double)m.y[R] + acc);
+        }
+    } else {
+        for (int t = t0 + (int)threadIdx.x; t < t1; t += blockDim.x)
+            fixup_in_chunk(m.tile_y, m.carry, t0, t1, nrow, m.y, t);
+    }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1) == G - 1);
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    for (int c = 1 + (int)threadIdx.x; c < G; c += blockDim.x) fixup_boundary(m.tile_y, m.carry, tile_num, chunk, nrow, m.y, c);
+    // crossing runs: one thread per boundary finishes a run of one carry
+    // tile (the common case: three independent loads, then y); longer runs
+    // are listed (in the free staging memory) and finished one warp each
+    int* s_long = reinterpret_cast<int*>(s_dyn);
+    if (threadIdx.x == 0) s_nlong = 0;
+    __syncthreads();
+    for (int c = 1 + (int)threadIdx.x; c < G; c += blockDim.x) {
+        const int b = start(c);
+        if (b <= 0 || b >= tile_num) continue;
+        const int R = open_row(m.tile_y, b - 1);
+        if (R >= nrow) continue;
+        const int r_prev = b >= 2 ? open_row(m.tile_y, b - 2) : -1;
+        const int r_next = open_row(m.tile_y, b);
+        if (r_prev == R || r_next == R) {
+            s_long[atomicAdd(&s_nlong, 1)] = c;
+            continue;
+        }
+        // the run is tile b - 1 alone and its row ends in tile b, finished
+        // here when tile b belongs to this chunk (an empty chunk leaves it
+        // to the next boundary, which has the same start)
+        if (b >= start(c + 1)) continue;
+        m.y[R] = (float)((double)__ldcg(m.y + R) + (double)__ldcg(m.carry + b - 1));
+    }
+    __syncthreads();
+    for (int i = warp; i < s_nlong; i += kPersistWarps) {
+        const int c = s_long[i];
+        fixup_boundary_warp(m.tile_y, m.carry, tile_num, start(c), start(c + 1), nrow, m.y, threadIdx.x & 31);
+    }
     if (threadIdx.x == 0) *ticket = 0;  // ready for the next launch
 }
 
@@ -323,7 +411,10 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
     m.hub = nullptr;
     m.gather_mode = p.gather_mode;
     const size_t stage = sizeof(float) * (size_t)kPersistWarps * tile_smem_words<SIGMA>();
-    const int grid = std::max(1, std::min(sm_count(), (p.tile_num + kPersistWarps - 1) / kPersistWarps));
+    const int grid = persistent_grid(p.tile_num);
+    // the plan's bounds were made for this grid (same device model); any
+    // other grid takes equal tile counts
+    const int32_t* bounds = (p.chunk_start && p.chunks == grid) ? p.chunk_start : nullptr;
     if (p.hub_k > 0) {
         const size_t smem = stage + sizeof(float) * (size_t)p.hub_k;
         static PerDeviceOnce once;
@@ -345,7 +436,8 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
         MR_CUDA_TRY(cudaFuncSetAttribute(merbit_persistent_kernel<V, SIGMA, true, GM>,
                                          cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         merbit_persistent_kernel<V, SIGMA, true, GM><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows,
-                                                                                        p.ticket, p.hub_cols, p.hub_k);
+                                                                                        p.ticket, p.hub_cols, p.hub_k,
+                                                                                        bounds);
     } else {
         static PerDeviceOnce once;
         MR_CUDA_TRY(once.run([&] {
@@ -360,7 +452,7 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
             return e;
         }));
         merbit_persistent_kernel<V, SIGMA, false, GM><<<grid, kPersistWarps * 32, stage, st>>>(m, p.tile_num, p.n_rows,
-                                                                                          p.ticket, nullptr, 0);
+                                                                                          p.ticket, nullptr, 0, bounds);
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
@@ -496,6 +588,71 @@ int build_hub_cache(MerbitPlan& p, const mr_csr_view& A, cudaStream_t st)
     MR_CUDA_TRY(cudaGetLastError());
     p.hub_k = (int)ncol;
     p.hub_coverage = coverage;
+    return MR_OK;
+}
+
+int persistent_grid(int tile_num)
+{
+    return std::max(1, std::min(sm_count(), (tile_num + kPersistWarps - 1) / kPersistWarps));
+}
+
+// Estimated cost of each tile, one warp per tile: 8 per x gather that misses
+// the hub cache (an L2 access), 1 per nonzero (stream bytes and hub gathers)
+// and 8 per tile. On R-MAT s21 under equal tile counts the SMs' busy cycles
+// spread as their chunks' non-hub gathers do (max / mean 1.21 measured, 1.19
+// predicted); weights of 4 to 32 per miss time the same at s22.
+constexpr int kCostMiss = 8;
+constexpr int kCostTile = 8;
+
+__global__ void tile_cost_kernel(const uint32_t* __restrict__ tile_x, const int32_t* __restrict__ cols, int nnz,
+                                 int tile_num, int32_t* __restrict__ cost)
+{
+    const int lane = threadIdx.x & 31;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int ws = (gridDim.x * blockDim.x) >> 5;
+    for (int t = w; t < tile_num; t += ws) {
+        const int a = min((int)__ldg(tile_x + t), nnz);
+        const int b = min((int)__ldg(tile_x + t + 1), nnz);
+        int miss = 0;
+        for (int k = a + lane; k < b; k += 32) miss += __ldg(cols + k) >= 0 ? 1 : 0;
+        miss = __reduce_add_sync(0xffffffffu, miss);
+        if (lane == 0) cost[t] = kCostMiss * miss + (b - a) + kCostTile;
+    }
+}
+
+int build_chunk_bounds(MerbitPlan& p, const int* colidx, cudaStream_t st)
+{
+    const int G = persistent_grid(p.tile_num);
+    if (G < 2 || p.tile_num < 2 * G) return MR_OK;  // equal tile counts
+    const int* cols = p.hub_k > 0 ? p.colh : colidx;
+    DevBuf cost;
+    MR_TRY(cost.alloc(sizeof(int32_t) * (size_t)p.tile_num, st));
+    const int grid = (int)std::min<int64_t>(((int64_t)p.tile_num * 32 + 255) / 256, (int64_t)sm_count() * 16);
+    tile_cost_kernel<<<grid, 256, 0, st>>>(p.tile_x, cols, (int)p.nnz, p.tile_num, cost.as<int32_t>());
+    MR_CUDA_TRY(cudaGetLastError());
+    std::vector<int32_t> c((size_t)p.tile_num);
+    MR_CUDA_TRY(cudaMemcpyAsync(c.data(), cost.p, sizeof(int32_t) * c.size(), cudaMemcpyDeviceToHost, st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));
+    // chunk g starts at the first tile whose cost prefix reaches g / G of the total
+    std::vector<int64_t> pre((size_t)p.tile_num + 1, 0);
+    for (int t = 0; t < p.tile_num; ++t) pre[(size_t)t + 1] = pre[(size_t)t] + c[(size_t)t];
+    const int64_t total = pre.back();
+    std::vector<int32_t> bounds((size_t)G + 1);
+    for (int g = 0; g <= G; ++g) {
+        const int64_t target = (int64_t)((__int128)total * g / G);
+        bounds[(size_t)g] = (int32_t)(std::lower_bound(pre.begin(), pre.end(), target) - pre.begin());
+    }
+    bounds[0] = 0;
+    bounds[(size_t)G] = p.tile_num;
+    if (cudaMalloc(&p.chunk_start, sizeof(int32_t) * bounds.size()) != cudaSuccess) {
+        cudaGetLastError();
+        p.chunk_start = nullptr;
+        return MR_OK;  // no room: equal tile counts
+    }
+    MR_CUDA_TRY(cudaMemcpyAsync(p.chunk_start, bounds.data(), sizeof(int32_t) * bounds.size(),
+                                cudaMemcpyHostToDevice, st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));  // the host vector goes out of scope
+    p.chunks = G;
     return MR_OK;
 }
 

@@ -138,6 +138,16 @@ def test_persistent_and_two_kernel_forms_bit_identical(M, cases, sigma):
     rp, ci, v = M.gen_rmat(scale=17, edge_factor=16, seed=8)
     big = dict(cases)
     big["rmat17"] = (rp, ci, v)
+    # 1,050,000 empty rows, then 10 rows of 1,300 nonzeros: the cost-balanced
+    # chunks of the persistent kernel are empty around each dense tile (17 to
+    # 54 of them, by SIGMA, on 148 SMs), and the dense rows' carry runs cross
+    # those empty chunks
+    rng = np.random.default_rng(4)
+    ne, nd, L = 1050000, 10, 1300
+    lens = np.concatenate([np.zeros(ne, np.int64), np.full(nd, L, np.int64)])
+    rp_d = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci_d = np.concatenate([np.sort(rng.choice(ne + nd, L, replace=False)) for _ in range(nd)]).astype(np.int32)
+    big["empty_then_dense"] = (rp_d, ci_d, rng.uniform(-1, 1, ci_d.size).astype(np.float32))
     for name, (rp, ci, v) in big.items():
         ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
         x = M.uniform(ncols, seed=2)
