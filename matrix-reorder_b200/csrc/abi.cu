@@ -150,6 +150,8 @@ int mr_merbit_plan_create_ex(const mr_csr_view* A, int sigma, int block, int fla
         cudaFree(p.colh);
         cudaFree(p.hub_cols);
         cudaFree(p.chunk_start);
+        cudaFree(p.boundary_run);
+        cudaFree(p.boundary_flag);
         delete h;
         return code;
     };
@@ -195,6 +197,8 @@ int mr_merbit_plan_destroy(mr_merbit_plan* h)
     cudaFree(h->p.colh);
     cudaFree(h->p.hub_cols);
     cudaFree(h->p.chunk_start);
+    cudaFree(h->p.boundary_run);
+    cudaFree(h->p.boundary_flag);
     if (dev != h->p.device) cudaSetDevice(dev);
     delete h;
     return MR_OK;

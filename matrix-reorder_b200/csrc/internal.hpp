@@ -38,6 +38,13 @@ struct MerbitPlan {
     // balanced by estimated cost (chunks + 1 entries); nullptr: equal tile counts
     int32_t* chunk_start = nullptr;
     int chunks = 0;
+    // the carry run that crosses the start of chunk c, c = 1 .. chunks - 1:
+    // {row, first tile, last tile, kind}; kind 0: none finishes in chunk c,
+    // 1: all its tiles lie in chunks c - 1 and c (finished by whichever of
+    // the two CTAs ends second), 2: it starts earlier (finished by the last
+    // CTA). chunks + 1 entries; boundary_flag: chunks + 1 arrival counters
+    int4* boundary_run = nullptr;
+    int* boundary_flag = nullptr;
 };
 
 int launch_merbit_plan(const int* rowptr, int nrow, int nnz, int sigma, int lane_num, int tile_num, uint32_t* tile_x,

@@ -232,13 +232,29 @@ __device__ __forceinline__ void fixup_boundary_warp(const uint32_t* __restrict__
     if (lane == 0) y[R] = (float)((double)__ldcg(y + R) + acc);
 }
 
+// Finishes a carry run known from the plan: carries of tiles u0 .. ue summed
+// in FP64 in tile order and added to y[R] (one warp).
+__device__ __forceinline__ void finish_run(const int4 run, const float* carry, float* y, int lane)
+{
+    const int R = run.x, u0 = run.y, ue = run.z;
+    const float yr = lane == 0 ? __ldcg(y + R) : 0.f;
+    double acc = 0.0;
+    for (int base = u0; base <= ue; base += 32) {
+        const float c = base + lane <= ue ? __ldcg(carry + base + lane) : 0.f;
+        const int cnt = min(32, ue - base + 1);
+        for (int j = 0; j < cnt; ++j) acc += (double)__shfl_sync(0xffffffffu, c, j);
+    }
+    if (lane == 0) y[R] = (float)((double)yr + acc);
+}
+
 template <typename V, int SIGMA, bool HUB, int GM>
 __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     merbit_persistent_kernel(const MerbitOperand<V, SIGMA> m_in, int tile_num, int nrow, int* __restrict__ ticket,
-                             const int32_t* __restrict__ hub_cols, int hub_k, const int32_t* __restrict__ chunk_start)
+                             const int32_t* __restrict__ hub_cols, int hub_k, const int32_t* __restrict__ chunk_start,
+                             const int4* __restrict__ brun, int* __restrict__ bflag)
 {
     extern __shared__ __align__(16) float s_dyn[];
-    __shared__ int s_last, s_nlong;
+    __shared__ int s_last, s_nlong, s_arrive[2];
     const int warp = threadIdx.x >> 5;
     const int G = gridDim.x;
     const int chunk = (tile_num + G - 1) / G;
@@ -310,11 +326,44 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     }
     __threadfence();
     __syncthreads();
+    const int lane = threadIdx.x & 31;
+    if (brun) {
+        // runs that cross a chunk start and lie in the two chunks beside it:
+        // the second of the two CTAs to get here finishes the run
+        if (threadIdx.x == 0) {
+            const int c = blockIdx.x;
+            s_arrive[0] = c >= 1 ? atomicAdd(bflag + c, 1) : 0;
+            s_arrive[1] = c + 1 <= G - 1 ? atomicAdd(bflag + c + 1, 1) : 0;
+            __threadfence();
+        }
+        __syncthreads();
+        if (warp < 2 && s_arrive[warp] == 1) {
+            const int c = blockIdx.x + warp;
+            const int4 run = __ldg(brun + c);
+            if (run.w == 1) finish_run(run, m.carry, m.y, lane);
+            if (lane == 0) bflag[c] = 0;  // both have arrived: ready for the next launch
+        }
+        __threadfence();
+        __syncthreads();
+    }
     if (threadIdx.x == 0) s_last = (atomicAdd(ticket, 1) == G - 1);
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // crossing runs: one thread per boundary finishes a run of one carry
+    if (brun) {
+        // runs that start before the chunk ahead of their boundary
+        int* s_list = reinterpret_cast<int*>(s_dyn);
+        if (threadIdx.x == 0) s_nlong = 0;
+        __syncthreads();
+        for (int c = 1 + (int)threadIdx.x; c < G; c += blockDim.x)
+            if (__ldg(&brun[c].w) == 2) s_list[atomicAdd(&s_nlong, 1)] = c;
+        __syncthreads();
+        for (int i = warp; i < s_nlong; i += kPersistWarps) finish_run(__ldg(brun + s_list[i]), m.carry, m.y, lane);
+        if (threadIdx.x == 0) *ticket = 0;  // ready for the next launch
+        return;
+    }
+    // plans without a run table (equal tile counts): the last CTA finishes
+    // every crossing run; one thread per boundary finishes a run of one carry
     // tile (the common case: three independent loads, then y); longer runs
     // are listed (in the free staging memory) and finished one warp each
     int* s_long = reinterpret_cast<int*>(s_dyn);
@@ -340,7 +389,7 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     __syncthreads();
     for (int i = warp; i < s_nlong; i += kPersistWarps) {
         const int c = s_long[i];
-        fixup_boundary_warp(m.tile_y, m.carry, tile_num, start(c), start(c + 1), nrow, m.y, threadIdx.x & 31);
+        fixup_boundary_warp(m.tile_y, m.carry, tile_num, start(c), start(c + 1), nrow, m.y, lane);
     }
     if (threadIdx.x == 0) *ticket = 0;  // ready for the next launch
 }
@@ -414,7 +463,10 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
     const int grid = persistent_grid(p.tile_num);
     // the plan's bounds were made for this grid (same device model); any
     // other grid takes equal tile counts
-    const int32_t* bounds = (p.chunk_start && p.chunks == grid) ? p.chunk_start : nullptr;
+    const bool own = p.chunk_start && p.chunks == grid;
+    const int32_t* bounds = own ? p.chunk_start : nullptr;
+    const int4* brun = own ? p.boundary_run : nullptr;
+    int* bflag = own ? p.boundary_flag : nullptr;
     if (p.hub_k > 0) {
         const size_t smem = stage + sizeof(float) * (size_t)p.hub_k;
         static PerDeviceOnce once;
@@ -437,7 +489,7 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
                                          cudaFuncAttributePreferredSharedMemoryCarveout, pct));
         merbit_persistent_kernel<V, SIGMA, true, GM><<<grid, kPersistWarps * 32, smem, st>>>(m, p.tile_num, p.n_rows,
                                                                                         p.ticket, p.hub_cols, p.hub_k,
-                                                                                        bounds);
+                                                                                        bounds, brun, bflag);
     } else {
         static PerDeviceOnce once;
         MR_CUDA_TRY(once.run([&] {
@@ -452,7 +504,8 @@ static int launch_persistent(const MerbitPlan& p, const int* colidx, const void*
             return e;
         }));
         merbit_persistent_kernel<V, SIGMA, false, GM><<<grid, kPersistWarps * 32, stage, st>>>(m, p.tile_num, p.n_rows,
-                                                                                          p.ticket, nullptr, 0, bounds);
+                                                                                          p.ticket, nullptr, 0, bounds,
+                                                                                          brun, bflag);
     }
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
@@ -644,14 +697,48 @@ int build_chunk_bounds(MerbitPlan& p, const int* colidx, cudaStream_t st)
     }
     bounds[0] = 0;
     bounds[(size_t)G] = p.tile_num;
-    if (cudaMalloc(&p.chunk_start, sizeof(int32_t) * bounds.size()) != cudaSuccess) {
-        cudaGetLastError();
+    // the carry run crossing each chunk start (the same runs, found the same
+    // way, as the kernel's boundary pass over tile_y)
+    std::vector<uint32_t> ty((size_t)p.tile_num + 1);
+    MR_CUDA_TRY(cudaMemcpy(ty.data(), p.tile_y, sizeof(uint32_t) * ty.size(), cudaMemcpyDeviceToHost));
+    auto orow = [&](int t) { return (int)(ty[(size_t)t + 1] & 0x7fffffffu); };
+    std::vector<int4> runs((size_t)G + 1, int4{0, 0, 0, 0});
+    for (int c = 1; c < G; ++c) {
+        const int a = bounds[(size_t)c - 1], b = bounds[(size_t)c], e = bounds[(size_t)c + 1];
+        if (b <= 0 || b >= p.tile_num || b >= e) continue;
+        const int R = orow(b - 1);
+        if (R >= p.n_rows) continue;
+        int ue = b - 1;
+        while (ue + 1 < p.tile_num && orow(ue + 1) == R) ++ue;
+        if (ue + 1 >= e) continue;  // the row ends in a later chunk
+        int u0 = b - 1;
+        while (u0 > 0 && orow(u0 - 1) == R) --u0;
+        runs[(size_t)c] = int4{R, u0, ue, (a < b && u0 >= a) ? 1 : 2};
+    }
+    auto release = [&] {
+        cudaFree(p.chunk_start);
+        cudaFree(p.boundary_run);
+        cudaFree(p.boundary_flag);
         p.chunk_start = nullptr;
+        p.boundary_run = nullptr;
+        p.boundary_flag = nullptr;
+    };
+    if (cudaMalloc(&p.chunk_start, sizeof(int32_t) * bounds.size()) != cudaSuccess ||
+        cudaMalloc(&p.boundary_run, sizeof(int4) * runs.size()) != cudaSuccess ||
+        cudaMalloc(&p.boundary_flag, sizeof(int) * runs.size()) != cudaSuccess) {
+        cudaGetLastError();
+        release();
         return MR_OK;  // no room: equal tile counts
     }
-    MR_CUDA_TRY(cudaMemcpyAsync(p.chunk_start, bounds.data(), sizeof(int32_t) * bounds.size(),
-                                cudaMemcpyHostToDevice, st));
-    MR_CUDA_TRY(cudaStreamSynchronize(st));  // the host vector goes out of scope
+    if (cudaMemcpyAsync(p.chunk_start, bounds.data(), sizeof(int32_t) * bounds.size(), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(p.boundary_run, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemsetAsync(p.boundary_flag, 0, sizeof(int) * runs.size(), st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {  // the host vectors go out of scope
+        release();
+        return MR_ERR_CUDA;
+    }
     p.chunks = G;
     return MR_OK;
 }
