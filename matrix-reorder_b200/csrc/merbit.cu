@@ -21,6 +21,12 @@
 //    partial sum of the row still open at the tile end goes to a per-tile
 //    carry slot, and a second kernel adds each run of carries to its row in
 //    FP64 in tile order. Results are bitwise reproducible run to run.
+//  * persistent form (block 1024): one CTA per SM over a chunk of tiles cut
+//    at plan time by estimated cost, with the hub cache of the hottest x
+//    columns in shared memory and the carry fix-up fused (runs inside a
+//    chunk walked in shared memory, runs across chunk starts finished from
+//    a plan-time table by the later of the two neighbouring CTAs): one
+//    launch per SpMV, bit-identical to the two-kernel form.
 #include <algorithm>
 #include <mutex>
 #include <vector>
