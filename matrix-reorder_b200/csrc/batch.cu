@@ -92,11 +92,28 @@ template <typename V, int SIGMA>
 __global__ void batch_fixup_kernel(const BatchOp<V, SIGMA>* __restrict__ ops, const long long* __restrict__ prefix,
                                    int count, long long total_tiles)
 {
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total_tiles;
-         g += (long long)gridDim.x * blockDim.x) {
-        const int it = find_item(prefix, count, g);
-        const BatchOp<V, SIGMA>& op = ops[it];
-        merbit_fixup_tile(op.m.tile_y, op.m.carry, op.tile_num, op.n_rows, op.m.y, (int)(g - __ldg(prefix + it)));
+    // warps step over the tiles 32 at a time (the loop is warp-uniform): a
+    // lane finishes the short run starting at its tile, then the warp
+    // finishes its lanes' long runs together
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = ((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5) * 32; base < total_tiles;
+         base += warps * 32) {
+        const long long g = base + lane;
+        int it = 0, t = 0, kind = 0;
+        if (g < total_tiles) {
+            it = find_item(prefix, count, g);
+            t = (int)(g - __ldg(prefix + it));
+            const BatchOp<V, SIGMA>& op = ops[it];
+            kind = fixup_run_short(op.m.tile_y, op.m.carry, op.tile_num, op.n_rows, op.m.y, t);
+        }
+        unsigned long_runs = __ballot_sync(0xffffffffu, kind == 2);
+        while (long_runs) {
+            const int src = __ffs(long_runs) - 1;
+            long_runs &= long_runs - 1;
+            const BatchOp<V, SIGMA>& op = ops[__shfl_sync(0xffffffffu, it, src)];
+            fixup_run_warp(op.m.tile_y, op.m.carry, op.tile_num, op.m.y, __shfl_sync(0xffffffffu, t, src), lane);
+        }
     }
 }
 

@@ -400,11 +400,20 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     if (threadIdx.x == 0) *ticket = 0;  // ready for the next launch
 }
 
+// One thread per tile finishes the short runs that start at its tile; the
+// warp then finishes its lanes' long runs together (whole warps: the grid
+// covers the tiles in blocks of 256).
 __global__ void merbit_fixup_kernel(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
                                     int tile_num, int nrow, float* __restrict__ y)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < tile_num) merbit_fixup_tile(tile_y, carry, tile_num, nrow, y, t);
+    const int kind = t < tile_num ? fixup_run_short(tile_y, carry, tile_num, nrow, y, t) : 0;
+    unsigned long_runs = __ballot_sync(0xffffffffu, kind == 2);
+    while (long_runs) {
+        const int src = __ffs(long_runs) - 1;
+        long_runs &= long_runs - 1;
+        fixup_run_warp(tile_y, carry, tile_num, y, __shfl_sync(0xffffffffu, t, src), threadIdx.x & 31);
+    }
 }
 
 template <typename V, int SIGMA, int WARPS>

@@ -244,22 +244,65 @@ __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, co
     __syncwarp();  // the warp may reuse s for its next tile
 }
 
-// Adds each run of carries to its row: the thread of the first tile of a run
-// of tiles whose open row at the tile end is the same row R sums their
-// carries in FP64, in tile order, and finishes y[R].
-__device__ __forceinline__ void merbit_fixup_tile(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
-                                                  int tile_num, int nrow, float* __restrict__ y, int t)
+// Carry runs. A run is the tiles t, t+1, ... whose row still open at the
+// tile end is the same row R (tile_y[u + 1] == R); their carries are added
+// to y[R] in FP64 in tile order, once the tile where R ends has written it.
+__device__ __forceinline__ int tile_open_row(const uint32_t* __restrict__ tile_y, int t)
 {
-    const int R = (int)(__ldg(tile_y + t + 1) & 0x7fffffffu);
-    if (R >= nrow) return;
-    if (t > 0 && (int)(__ldg(tile_y + t) & 0x7fffffffu) == R) return;  // not the first tile of the run
+    return (int)(__ldg(tile_y + t + 1) & 0x7fffffffu);
+}
+
+constexpr int kShortRun = 8;
+
+// For tile t: 0 if it does not start a run; 1 if it starts a run of at most
+// kShortRun tiles, now finished (the open rows and carries of the next tiles
+// are loaded together, then summed in order); 2 if it starts a longer run,
+// left to fixup_run_warp.
+__device__ __forceinline__ int fixup_run_short(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
+                                               int tile_num, int nrow, float* __restrict__ y, int t)
+{
+    const int R = tile_open_row(tile_y, t);
+    if (R >= nrow) return 0;
+    if (t > 0 && tile_open_row(tile_y, t - 1) == R) return 0;  // not the first tile of its run
+    int len = 1;
+#pragma unroll
+    for (int j = 1; j <= kShortRun; ++j) {
+        const bool same = t + j < tile_num && tile_open_row(tile_y, t + j) == R;
+        if (same && len == j) len = j + 1;
+    }
+    if (len > kShortRun) return 2;
     double acc = 0.0;
-    int u = t;
-    do {
-        acc += (double)carry[u];
-        ++u;
-    } while (u < tile_num && (int)(__ldg(tile_y + u + 1) & 0x7fffffffu) == R);
+#pragma unroll
+    for (int j = 0; j < kShortRun; ++j)
+        if (j < len) acc += (double)__ldg(carry + t + j);
     y[R] = (float)((double)y[R] + acc);
+    return 1;
+}
+
+// The run starting at tile t, by the whole warp: its end found 32 tiles per
+// step with ballots (open rows never decrease along the tiles), its carries
+// loaded 32 at a time and summed in FP64 in tile order through shuffles.
+__device__ __forceinline__ void fixup_run_warp(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
+                                               int tile_num, float* __restrict__ y, int t, int lane)
+{
+    const int R = tile_open_row(tile_y, t);
+    int ue = t;
+    for (;;) {
+        const int q = ue + 1 + lane;
+        const unsigned m = __ballot_sync(0xffffffffu, q < tile_num && tile_open_row(tile_y, q) == R);
+        if (m != 0xffffffffu) {
+            ue += __ffs(~m) - 1;
+            break;
+        }
+        ue += 32;
+    }
+    double acc = 0.0;
+    for (int base = t; base <= ue; base += 32) {
+        const float c = base + lane <= ue ? __ldg(carry + base + lane) : 0.f;
+        const int cnt = min(32, ue - base + 1);
+        for (int j = 0; j < cnt; ++j) acc += (double)__shfl_sync(0xffffffffu, c, j);
+    }
+    if (lane == 0) y[R] = (float)((double)y[R] + acc);
 }
 
 }  // namespace mr
