@@ -141,7 +141,10 @@ int mr_merbit_plan_get_info(const mr_merbit_plan* plan, mr_merbit_plan_info* inf
  * loop of GRAPH::spmv(env, "merbit") (src/class.cu:1407-1430,
  * include/merbit.cuh:408-493). Deterministic: rows spanning tiles are
  * finished by an FP64 carry fix-up instead of float atomics, so no second
- * output buffer (the reference's d_z) is needed. */
+ * output buffer (the reference's d_z) is needed. A call uses the plan's
+ * carry slots and completion counters: calls with the same plan must not
+ * overlap on the GPU (order them on one stream or with events); calls with
+ * different plans may. */
 int mr_spmv_merbit(const mr_merbit_plan* plan, const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
 
 /* Allocation-free MERBIT SpMV: y = A x with no device allocation at all.
