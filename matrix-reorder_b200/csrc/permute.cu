@@ -506,23 +506,36 @@ __device__ __forceinline__ void cta_sort_any(int cnt, int src, int start, const 
         cta_sort_segment<16>(cnt, src, start, colidx, perm, s, sink);
 }
 
-// rows of length (256, 4096]: one 256-thread CTA per row (grid-stride over the list)
-template <typename E>
-__global__ void __launch_bounds__(256, 2)
+// rows of length (256, 4096]: one 256-thread CTA per row (grid-stride over
+// the list). Two instantiations: rows of at most kMedSmall keys with a small
+// buffer and 6 CTAs per SM, the longer ones with the full buffer at 2 per SM
+// (each skips the other's rows).
+constexpr int kMedSmall = 1024;
+
+template <typename E, int MAXLEN>
+__global__ void __launch_bounds__(256, MAXLEN <= kMedSmall ? 6 : 2)
     sort_med_rows_kernel(const int32_t* __restrict__ list, int count, const int32_t* __restrict__ rowptr,
                          const int32_t* __restrict__ colidx, const E* __restrict__ vals,
                          const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
                          const int32_t* __restrict__ out_rowptr, int32_t* __restrict__ out_col,
                          E* __restrict__ out_val)
 {
-    __shared__ unsigned long long s[kMedRow];
+    __shared__ unsigned long long s[MAXLEN];
     for (int r = blockIdx.x; r < count; r += gridDim.x) {
         const int i = list[r];
         const int dst = out_rowptr[i];
         const int len = out_rowptr[i + 1] - dst;
+        if ((len <= kMedSmall) != (MAXLEN <= kMedSmall)) continue;  // the other instantiation's row
         const int src = rowptr[inv[i]];
         // sorted keys back to shared memory, then a coalesced emit
-        cta_sort_any(len, src, 0, colidx, perm, s, [&](int t, unsigned long long key) { s[t] = key; });
+        if constexpr (MAXLEN <= kMedSmall) {
+            if (len <= 512)
+                cta_sort_segment<2>(len, src, 0, colidx, perm, s, [&](int t, unsigned long long key) { s[t] = key; });
+            else
+                cta_sort_segment<4>(len, src, 0, colidx, perm, s, [&](int t, unsigned long long key) { s[t] = key; });
+        } else {
+            cta_sort_any(len, src, 0, colidx, perm, s, [&](int t, unsigned long long key) { s[t] = key; });
+        }
         __syncthreads();
         for (int t = threadIdx.x; t < len; t += blockDim.x) emit_sorted<E>(s[t], dst + t, src, vals, out_col, out_val);
         __syncthreads();
@@ -572,45 +585,68 @@ __global__ void __launch_bounds__(256, 2)
     }
 }
 
-// One merge pass: runs of width w are merged pairwise, in[] -> out[] (or,
-// on the last pass, straight into the output CSR). Each thread produces 16
-// consecutive outputs of its tile, starting at its merge-path co-rank.
+// How many of the first d outputs of merging a[0, na) and b[0, nb) come
+// from a (keys are unique: the source position breaks column ties).
+__device__ __forceinline__ int merge_co_rank(const unsigned long long* a, int na, const unsigned long long* b, int nb,
+                                             int d)
+{
+    int alo = max(0, d - nb), ahi = min(d, na);
+    while (alo < ahi) {
+        const int am = (alo + ahi) >> 1;
+        if (a[am] < b[d - am - 1])
+            alo = am + 1;
+        else
+            ahi = am;
+    }
+    return alo;
+}
+
+// One merge pass: runs of width w are merged pairwise, in[] -> out[]; a
+// row whose length is at most 2w is finished by this pass and written
+// straight into the output CSR, and a row of at most w was finished by an
+// earlier pass and is skipped. Per tile of 4096 outputs, the two input
+// ranges it draws from (found by two co-rank searches) are staged in shared
+// memory; each thread then merges its 16 consecutive outputs there.
 template <typename E>
 __global__ void __launch_bounds__(256)
     long_merge_kernel(const LongTile* __restrict__ tiles, int ntiles, const LongRow* __restrict__ rows, int w,
-                      const unsigned long long* __restrict__ in, unsigned long long* __restrict__ out, int last,
+                      const unsigned long long* __restrict__ in, unsigned long long* __restrict__ out,
                       const E* __restrict__ vals, int32_t* __restrict__ out_col, E* __restrict__ out_val)
 {
     constexpr int PER = kMedRow / 256;
+    __shared__ unsigned long long s_in[kMedRow];
+    __shared__ int s_ia[2];
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const LongTile tl = tiles[t];
         const LongRow R = rows[tl.row];
+        if (R.len <= w) continue;  // finished by an earlier pass (uniform over the CTA)
+        const bool last = R.len <= 2 * w;
         const int lo = tl.start / (2 * w) * (2 * w);
         const int mid = min(lo + w, R.len), hi = min(lo + 2 * w, R.len);
         const int na = mid - lo, nb = hi - mid;
         const unsigned long long* a = in + R.soff + lo;
         const unsigned long long* b = in + R.soff + mid;
-        const int d0 = tl.start - lo + (int)threadIdx.x * PER;
-        const int d1 = min(d0 + PER, min(tl.start + kMedRow, R.len) - lo);
-        if (d0 >= d1) continue;
-        // co-rank: how many of the first d0 outputs come from a
-        int alo = max(0, d0 - nb), ahi = min(d0, na);
-        while (alo < ahi) {
-            const int am = (alo + ahi) >> 1;
-            if (a[am] < b[d0 - am - 1])
-                alo = am + 1;
-            else
-                ahi = am;
+        const int D0 = tl.start - lo, D1 = min(tl.start + kMedRow, R.len) - lo;  // this tile's outputs
+        if (threadIdx.x < 2) s_ia[threadIdx.x] = merge_co_rank(a, na, b, nb, threadIdx.x == 0 ? D0 : D1);
+        __syncthreads();
+        const int ia0 = s_ia[0], ia1 = s_ia[1];
+        const int ib0 = D0 - ia0, ib1 = D1 - ia1;
+        const int ta = ia1 - ia0, tb = ib1 - ib0;  // ta + tb = D1 - D0 <= kMedRow
+        for (int u = threadIdx.x; u < ta + tb; u += blockDim.x) s_in[u] = u < ta ? a[ia0 + u] : b[ib0 + u - ta];
+        __syncthreads();
+        const int d0 = (int)threadIdx.x * PER, d1 = min(d0 + PER, ta + tb);
+        if (d0 < d1) {
+            int ia = merge_co_rank(s_in, ta, s_in + ta, tb, d0), ib = d0 - ia;
+            for (int d = d0; d < d1; ++d) {
+                const bool takeA = ib >= tb || (ia < ta && s_in[ia] < s_in[ta + ib]);
+                const unsigned long long key = takeA ? s_in[ia++] : s_in[ta + ib++];
+                if (last)
+                    emit_sorted<E>(key, R.dst + lo + D0 + d, R.src, vals, out_col, out_val);
+                else
+                    out[R.soff + lo + D0 + d] = key;
+            }
         }
-        int ia = alo, ib = d0 - alo;
-        for (int d = d0; d < d1; ++d) {
-            const bool takeA = ib >= nb || (ia < na && a[ia] < b[ib]);
-            const unsigned long long key = takeA ? a[ia++] : b[ib++];
-            if (last)
-                emit_sorted<E>(key, R.dst + lo + d, R.src, vals, out_col, out_val);
-            else
-                out[R.soff + lo + d] = key;
-        }
+        __syncthreads();  // s_in is reused by the next tile
     }
 }
 
@@ -646,9 +682,8 @@ static int sort_long_rows(const mr_csr_view& A, const int32_t* perm, const int32
     MR_CUDA_TRY(cudaGetLastError());
     const E* v = reinterpret_cast<const E*>(A.vals);
     for (int w = kMedRow; w < hs.max_len; w <<= 1) {
-        const int last = 2 * w >= hs.max_len;
-        long_merge_kernel<E><<<grid, 256, 0, st>>>(tiles_d.as<LongTile>(), nt, rows_d.as<LongRow>(), w, bufA, bufB, last,
-                                                 v, out_col, out_val);
+        long_merge_kernel<E><<<grid, 256, 0, st>>>(tiles_d.as<LongTile>(), nt, rows_d.as<LongRow>(), w, bufA, bufB, v,
+                                                 out_col, out_val);
         MR_CUDA_TRY(cudaGetLastError());
         std::swap(bufA, bufB);
     }
@@ -672,9 +707,12 @@ static int launch_sorts(const mr_csr_view& A, const int32_t* perm, const int32_t
         sort_warp_rows_kernel<E><<<g, 256, 0, st>>>(warp_list, hs.n_warp, A.rowptr, A.colidx, v, perm, inv, out_rowptr,
                                                    out_col, ov);
     }
-    if (hs.n_med > 0)
-        sort_med_rows_kernel<E><<<std::min(hs.n_med, sm_count() * 8), 256, 0, st>>>(
+    if (hs.n_med > 0) {
+        sort_med_rows_kernel<E, kMedSmall><<<std::min(hs.n_med, sm_count() * 12), 256, 0, st>>>(
             med, hs.n_med, A.rowptr, A.colidx, v, perm, inv, out_rowptr, out_col, ov);
+        sort_med_rows_kernel<E, kMedRow><<<std::min(hs.n_med, sm_count() * 8), 256, 0, st>>>(
+            med, hs.n_med, A.rowptr, A.colidx, v, perm, inv, out_rowptr, out_col, ov);
+    }
     MR_CUDA_TRY(cudaGetLastError());
     if (hs.n_large > 0) MR_TRY(sort_long_rows<E>(A, perm, inv, out_rowptr, out_col, ov, hs, large, st));
     return MR_OK;
