@@ -247,6 +247,7 @@ int validate_csr(const mr_csr_view& A, int* ok, cudaStream_t st)
 
 // --------------------------------------------------------- CSR permute ----
 
+constexpr int kTinyRow = 8;     // one thread, a sorting network in registers
 constexpr int kSmallRow = 32;   // one warp, one key per lane
 constexpr int kWarpRow = 256;   // one warp, up to 8 keys per lane in registers
 constexpr int kMedRow = 4096;   // one CTA, shared-memory bitonic; longer rows: chunks + merge passes
@@ -255,6 +256,7 @@ struct PermStats {
     int bad;
     int bad_csr;
     int max_len;
+    int n_small;
     int n_warp;
     int n_med;
     int n_large;
@@ -264,8 +266,9 @@ struct PermStats {
 // new row lengths and the lists of rows that need more than one key per
 // lane (warp-aggregated appends: one atomic per warp and list)
 __global__ void row_lengths_kernel(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ inv,
-                                   int32_t* __restrict__ len, PermStats* stats, int32_t* __restrict__ warp_list,
-                                   int32_t* __restrict__ med_list, int32_t* __restrict__ large_list)
+                                   int32_t* __restrict__ len, PermStats* stats, int32_t* __restrict__ small_list,
+                                   int32_t* __restrict__ warp_list, int32_t* __restrict__ med_list,
+                                   int32_t* __restrict__ large_list)
 {
     const int lane = threadIdx.x & 31;
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -276,17 +279,20 @@ __global__ void row_lengths_kernel(int n, const int32_t* __restrict__ rowptr, co
             if (o >= 0 && o < n) l = rowptr[o + 1] - rowptr[o];
             len[i] = l;
         }
-        const int cls = (i >= n || l <= kSmallRow) ? 0 : (l <= kWarpRow ? 1 : (l <= kMedRow ? 2 : 3));
+        // 0: empty or at most kTinyRow keys (no list: the tiny kernel visits every row)
+        const int cls = (i >= n || l <= kTinyRow)
+                            ? 0
+                            : (l <= kSmallRow ? 4 : (l <= kWarpRow ? 1 : (l <= kMedRow ? 2 : 3)));
         if (cls == 3) {
             atomicMax(&stats->max_len, l);
             atomicAdd(&stats->large_total, (unsigned long long)l);
         }
 #pragma unroll
-        for (int c = 1; c <= 3; ++c) {
+        for (int c = 1; c <= 4; ++c) {
             const unsigned m = __ballot_sync(0xffffffffu, cls == c);
             if (!m) continue;
-            int* counter = c == 1 ? &stats->n_warp : (c == 2 ? &stats->n_med : &stats->n_large);
-            int32_t* list = c == 1 ? warp_list : (c == 2 ? med_list : large_list);
+            int* counter = c == 1 ? &stats->n_warp : (c == 2 ? &stats->n_med : (c == 3 ? &stats->n_large : &stats->n_small));
+            int32_t* list = c == 1 ? warp_list : (c == 2 ? med_list : (c == 3 ? large_list : small_list));
             const int leader = __ffs(m) - 1;
             int b = 0;
             if (lane == leader) b = atomicAdd(counter, __popc(m));
@@ -313,32 +319,89 @@ __device__ __forceinline__ void emit_sorted(unsigned long long key, int dst, int
 }
 
 // rows of length <= 32: one warp per row, bitonic network in registers
+// compare-exchange: a <= b afterwards
+__device__ __forceinline__ void cx(unsigned long long& a, unsigned long long& b)
+{
+    const unsigned long long lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+
+// rows of 1 .. kTinyRow keys: one thread per row, keys padded with ~0 to a
+// sorting network of 4 (5 exchanges) or 8 (19 exchanges, Batcher's
+// odd-even merge sort) in registers
 template <typename E>
 __global__ void __launch_bounds__(256)
-    sort_small_rows_kernel(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colidx,
-                           const E* __restrict__ vals, const int32_t* __restrict__ perm,
-                           const int32_t* __restrict__ inv, const int32_t* __restrict__ out_rowptr,
-                           int32_t* __restrict__ out_col, E* __restrict__ out_val)
+    sort_tiny_rows_kernel(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colidx,
+                          const E* __restrict__ vals, const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
+                          const int32_t* __restrict__ out_rowptr, int32_t* __restrict__ out_col,
+                          E* __restrict__ out_val)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int dst = out_rowptr[i];
+        const int len = out_rowptr[i + 1] - dst;
+        if (len == 0 || len > kTinyRow) continue;
+        const int src = rowptr[inv[i]];
+        unsigned long long k[kTinyRow];
+#pragma unroll
+        for (int j = 0; j < kTinyRow; ++j) k[j] = j < len ? perm_key(perm, colidx, src, j) : ~0ull;
+        if (len > 1) {
+            cx(k[0], k[1]);
+            cx(k[2], k[3]);
+            cx(k[0], k[2]);
+            cx(k[1], k[3]);
+            cx(k[1], k[2]);
+            if (len > 4) {
+                cx(k[4], k[5]);
+                cx(k[6], k[7]);
+                cx(k[4], k[6]);
+                cx(k[5], k[7]);
+                cx(k[5], k[6]);
+                // merge the two sorted halves
+                cx(k[0], k[4]);
+                cx(k[1], k[5]);
+                cx(k[2], k[6]);
+                cx(k[3], k[7]);
+                cx(k[2], k[4]);
+                cx(k[3], k[5]);
+                cx(k[1], k[2]);
+                cx(k[3], k[4]);
+                cx(k[5], k[6]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kTinyRow; ++j)
+            if (j < len) emit_sorted<E>(k[j], dst + j, src, vals, out_col, out_val);
+    }
+}
+
+// rows of kTinyRow+1 .. kSmallRow keys (listed): one warp each, one key per
+// lane, a register bitonic network over the warp
+template <typename E>
+__global__ void __launch_bounds__(256)
+    sort_small_rows_kernel(const int32_t* __restrict__ list, int count, const int32_t* __restrict__ rowptr,
+                           const int32_t* __restrict__ colidx, const E* __restrict__ vals,
+                           const int32_t* __restrict__ perm, const int32_t* __restrict__ inv,
+                           const int32_t* __restrict__ out_rowptr, int32_t* __restrict__ out_col,
+                           E* __restrict__ out_val)
 {
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < count; r += warps) {
+        const int i = list[r];
         const int dst = out_rowptr[i];
         const int len = out_rowptr[i + 1] - dst;
-        if (len > kSmallRow || len == 0) continue;
         const int src = rowptr[inv[i]];
         unsigned long long key = ~0ull;
         if (lane < len) key = perm_key(perm, colidx, src, lane);
-        if (len > 1) {
 #pragma unroll
-            for (int k = 2; k <= 32; k <<= 1) {
+        for (int k = 2; k <= 32; k <<= 1) {
 #pragma unroll
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, j);
-                    const bool up = (lane & k) == 0;
-                    const bool lower = (lane & j) == 0;
-                    key = (lower == up) ? min(key, other) : max(key, other);
-                }
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, j);
+                const bool up = (lane & k) == 0;
+                const bool lower = (lane & j) == 0;
+                key = (lower == up) ? min(key, other) : max(key, other);
             }
         }
         if (lane < len) emit_sorted<E>(key, dst + lane, src, vals, out_col, out_val);
@@ -693,15 +756,19 @@ static int sort_long_rows(const mr_csr_view& A, const int32_t* perm, const int32
 
 template <typename E>
 static int launch_sorts(const mr_csr_view& A, const int32_t* perm, const int32_t* inv, const int32_t* out_rowptr,
-                        int32_t* out_col, void* out_val, const PermStats& hs, const int32_t* warp_list,
-                        const int32_t* med, const int32_t* large, cudaStream_t st)
+                        int32_t* out_col, void* out_val, const PermStats& hs, const int32_t* small_list,
+                        const int32_t* warp_list, const int32_t* med, const int32_t* large, cudaStream_t st)
 {
     const int n = A.n_rows;
     const E* v = reinterpret_cast<const E*>(A.vals);
     E* ov = reinterpret_cast<E*>(out_val);
-    const int grid_small = (int)std::min<int64_t>(((int64_t)n * 32 + 255) / 256, (int64_t)sm_count() * 32);
-    sort_small_rows_kernel<E><<<std::max(grid_small, 1), 256, 0, st>>>(n, A.rowptr, A.colidx, v, perm, inv, out_rowptr,
-                                                                       out_col, ov);
+    sort_tiny_rows_kernel<E><<<grid_for(n, 256), 256, 0, st>>>(n, A.rowptr, A.colidx, v, perm, inv, out_rowptr,
+                                                               out_col, ov);
+    if (hs.n_small > 0) {
+        const int g = (int)std::min<int64_t>(((int64_t)hs.n_small * 32 + 255) / 256, (int64_t)sm_count() * 32);
+        sort_small_rows_kernel<E><<<g, 256, 0, st>>>(small_list, hs.n_small, A.rowptr, A.colidx, v, perm, inv,
+                                                    out_rowptr, out_col, ov);
+    }
     if (hs.n_warp > 0) {
         const int g = (int)std::min<int64_t>(((int64_t)hs.n_warp * 32 + 255) / 256, (int64_t)sm_count() * 32);
         sort_warp_rows_kernel<E><<<g, 256, 0, st>>>(warp_list, hs.n_warp, A.rowptr, A.colidx, v, perm, inv, out_rowptr,
@@ -729,17 +796,18 @@ int permute_csr(const mr_csr_view& A, const int32_t* perm, int32_t* out_rowptr, 
     DevBuf inv, stats, lists, scan_ws;
     MR_TRY(inv.alloc(sizeof(int32_t) * (size_t)n, st));
     MR_TRY(stats.alloc(sizeof(PermStats), st));
-    MR_TRY(lists.alloc(sizeof(int32_t) * 3 * (size_t)n, st));
+    MR_TRY(lists.alloc(sizeof(int32_t) * 4 * (size_t)n, st));
     MR_TRY(scan_ws.alloc(scan_workspace_bytes(n), st));
     MR_CUDA_TRY(cudaMemsetAsync(stats.p, 0, sizeof(PermStats), st));
     PermStats* ds = stats.as<PermStats>();
     MR_TRY(launch_perm_invert(n, perm, inv.as<int32_t>(), &ds->bad, st));
     MR_TRY(validate_csr_async(A, &ds->bad_csr, st));
-    int32_t* warp_list = lists.as<int32_t>();
+    int32_t* small_list = lists.as<int32_t>();
+    int32_t* warp_list = small_list + n;
     int32_t* med = warp_list + n;
     int32_t* large = med + n;
-    row_lengths_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, A.rowptr, inv.as<int32_t>(), out_rowptr, ds, warp_list, med,
-                                                         large);
+    row_lengths_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, A.rowptr, inv.as<int32_t>(), out_rowptr, ds, small_list,
+                                                         warp_list, med, large);
     MR_CUDA_TRY(cudaGetLastError());
     MR_TRY(exclusive_scan_i32_ws(out_rowptr, out_rowptr, n, scan_ws.p, st));
     PermStats hs;
@@ -748,10 +816,10 @@ int permute_csr(const mr_csr_view& A, const int32_t* perm, int32_t* out_rowptr, 
     if (hs.bad_csr) return MR_ERR_INVALID_ARG;
     if (hs.bad) return MR_ERR_INVALID_PERM;
     if (A.dtype == MR_F32)
-        return launch_sorts<uint32_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, warp_list, med,
-                                      large, st);
-    return launch_sorts<uint16_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, warp_list, med,
-                                  large, st);
+        return launch_sorts<uint32_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, small_list,
+                                      warp_list, med, large, st);
+    return launch_sorts<uint16_t>(A, perm, inv.as<int32_t>(), out_rowptr, out_colidx, out_vals, hs, small_list,
+                                  warp_list, med, large, st);
 }
 
 }  // namespace mr
