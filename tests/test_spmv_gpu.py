@@ -158,6 +158,41 @@ def test_persistent_and_two_kernel_forms_bit_identical(M, cases, sigma):
         p2.close()
 
 
+def test_persistent_plan_replays_in_cuda_graph(M):
+    """The persistent kernel's completion ticket and chunk-boundary counters
+    are reset by the launch that uses them: a captured SpMV replayed many
+    times (and mixed with direct calls) gives the direct call's y bit for
+    bit every time."""
+    import torch
+    rp, ci, v = M.gen_rmat(scale=17, edge_factor=16, seed=8)
+    n = rp.size - 1
+    A = M.view(_dev(rp), _dev(ci), _dev(v))
+    x = _dev(M.uniform(n, seed=6))
+    plan = M.MerbitPlan(A, sigma=14, block=1024)
+    ref = torch.empty_like(x)
+    plan.spmv(x, ref)
+    torch.cuda.synchronize()
+    y = torch.full_like(x, float("nan"))
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        plan.spmv(x, y, stream=s)  # warm-up on the capture stream
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        plan.spmv(x, y, stream=torch.cuda.current_stream())
+    for k in range(20):
+        y.fill_(float("nan"))
+        g.replay()
+        if k % 5 == 4:
+            plan.spmv(x, y)  # direct calls between replays
+        torch.cuda.synchronize()
+        assert torch.equal(y.view(torch.int32), ref.view(torch.int32)), k
+    del g
+    plan.close()
+
+
 def test_hub_cache_bit_identical_and_reported(M):
     """The shared-memory hub cache changes where x comes from, not the
     arithmetic: results must equal the plan without it bit for bit. Skewed
