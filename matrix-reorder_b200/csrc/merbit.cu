@@ -166,17 +166,17 @@ __global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOpe
 // chunk bounds come from the plan, balanced by estimated cost (a tile's x
 // gathers that miss the hub cache dominate its time, so equal tile counts
 // leave some SMs working 20% longer than the mean), or are equal tile counts
-// when the plan has none. Rows whose carry run stays inside a chunk are
-// finished by the chunk's CTA after a barrier; the last CTA to finish
-// (atomic ticket after a fence) finishes the runs that cross chunk
-// boundaries. Same FP64 run sums, same order, as the two-kernel form: the
-// results are bit-identical.
+// when the plan has none. Carry runs that stay inside a chunk are finished
+// by the chunk's CTA after a barrier, walked in shared memory. A run that
+// crosses a chunk start is finished, from the plan's run table, by the
+// second of the two CTAs beside that start to get there (arrival counters,
+// no waiting), or, when it starts before the previous chunk, by the last CTA
+// to finish (atomic ticket after a fence); plans without a table leave
+// every crossing run to the last CTA. Same FP64 run sums, same order, as the
+// two-kernel form: the results are bit-identical.
 constexpr int kPersistWarps = 32;
 
-__device__ __forceinline__ int open_row(const uint32_t* tile_y, int t)
-{
-    return (int)(__ldg(tile_y + t + 1) & 0x7fffffffu);
-}
+__device__ __forceinline__ int open_row(const uint32_t* tile_y, int t) { return tile_open_row(tile_y, t); }
 
 // run that starts in [t0, t1) and whose row ends inside the chunk
 __device__ __forceinline__ void fixup_in_chunk(const uint32_t* __restrict__ tile_y, const float* carry, int t0, int t1,
