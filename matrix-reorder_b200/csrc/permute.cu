@@ -265,11 +265,16 @@ struct PermStats {
 
 // new row lengths and the lists of rows that need more than one key per
 // lane (warp-aggregated appends: one atomic per warp and list)
-__global__ void row_lengths_kernel(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ inv,
-                                   int32_t* __restrict__ len, PermStats* stats, int32_t* __restrict__ small_list,
-                                   int32_t* __restrict__ warp_list, int32_t* __restrict__ med_list,
-                                   int32_t* __restrict__ large_list)
+__global__ void __launch_bounds__(256)
+    row_lengths_kernel(int n, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ inv,
+                       int32_t* __restrict__ len, PermStats* stats, int32_t* __restrict__ small_list,
+                       int32_t* __restrict__ warp_list, int32_t* __restrict__ med_list,
+                       int32_t* __restrict__ large_list)
 {
+    // list appends: ranks within the warp (ballot), warp offsets within the
+    // CTA (shared counters), one global atomic per class and CTA step. The
+    // order of a list only decides which CTA sorts which row.
+    __shared__ int s_cnt[4], s_base[4];
     const int lane = threadIdx.x & 31;
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int i = base + (int)threadIdx.x;
@@ -287,18 +292,29 @@ __global__ void row_lengths_kernel(int n, const int32_t* __restrict__ rowptr, co
             atomicMax(&stats->max_len, l);
             atomicAdd(&stats->large_total, (unsigned long long)l);
         }
+        if (threadIdx.x < 4) s_cnt[threadIdx.x] = 0;
+        __syncthreads();
+        int warp_off[4], rank = 0;
 #pragma unroll
         for (int c = 1; c <= 4; ++c) {
             const unsigned m = __ballot_sync(0xffffffffu, cls == c);
-            if (!m) continue;
-            int* counter = c == 1 ? &stats->n_warp : (c == 2 ? &stats->n_med : (c == 3 ? &stats->n_large : &stats->n_small));
-            int32_t* list = c == 1 ? warp_list : (c == 2 ? med_list : (c == 3 ? large_list : small_list));
-            const int leader = __ffs(m) - 1;
-            int b = 0;
-            if (lane == leader) b = atomicAdd(counter, __popc(m));
-            b = __shfl_sync(0xffffffffu, b, leader);
-            if (cls == c) list[b + __popc(m & ((1u << lane) - 1u))] = i;
+            int off = 0;
+            if (m && lane == __ffs(m) - 1) off = atomicAdd(&s_cnt[c - 1], __popc(m));
+            warp_off[c - 1] = __shfl_sync(0xffffffffu, off, m ? __ffs(m) - 1 : 0);
+            if (cls == c) rank = __popc(m & ((1u << lane) - 1u));
         }
+        __syncthreads();
+        if (threadIdx.x < 4 && s_cnt[threadIdx.x] > 0) {
+            const int c = threadIdx.x + 1;
+            int* counter = c == 1 ? &stats->n_warp : (c == 2 ? &stats->n_med : (c == 3 ? &stats->n_large : &stats->n_small));
+            s_base[threadIdx.x] = atomicAdd(counter, s_cnt[threadIdx.x]);
+        }
+        __syncthreads();
+        if (cls > 0) {
+            int32_t* list = cls == 1 ? warp_list : (cls == 2 ? med_list : (cls == 3 ? large_list : small_list));
+            list[s_base[cls - 1] + warp_off[cls - 1] + rank] = i;
+        }
+        __syncthreads();  // s_cnt / s_base are reset by the next step
     }
 }
 
