@@ -112,10 +112,11 @@ typedef struct mr_merbit_plan_info {
 } mr_merbit_plan_info;
 
 /* block 1024 (the default) selects the persistent kernel: one CTA of 32
- * warps per SM sweeping a contiguous range of tiles, with the carry fix-up
- * fused in. Its plan also builds a hub cache when it pays: the most-used
- * columns (as many as fit in shared memory beside the staging buffers, and
- * only if they take >= 25% of the nonzeros) are staged in shared memory at
+ * warps per SM sweeping a contiguous range of tiles (ranges cut at plan
+ * time by estimated cost), with the carry fix-up fused in. Its plan also
+ * builds a hub cache when it pays: the most-used columns (as many as fit in
+ * shared memory beside the staging buffers, and only if they take >= 20% of
+ * the nonzeros) are staged in shared memory at
  * kernel start, and the plan keeps a copy of colidx with those columns
  * remapped — so such a plan snapshots the column indices of A, and must be
  * rebuilt if they change. block 128/256/512 select the tile-per-warp grid
