@@ -50,11 +50,11 @@ __device__ __forceinline__ int find_item(const long long* __restrict__ prefix, i
     return lo;
 }
 
-// One 1024-thread CTA per SM; CTA b sweeps the contiguous chunk b of the
-// concatenated tile space, its warps taking every 32nd tile, so the warps of
-// an SM work on neighbouring tiles of the same item (x reuse in L1, the
-// streams bypass L1 and leave L2 first). A warp looks its item up again only
-// when its tile leaves the current item.
+// One 1024-thread CTA per SM over the concatenated tile space of the group's
+// items, in 32-tile sub-chunks (one tile per warp), so the warps of an SM
+// work on neighbouring tiles of the same item (x reuse in L1, the streams
+// bypass L1 and leave L2 first). A warp looks its item up again only when
+// its tile leaves the current item.
 constexpr int kBatchWarps = 32;
 
 template <typename V, int SIGMA>
@@ -66,12 +66,19 @@ __global__ void __launch_bounds__(kBatchWarps * 32, 1)
     const int warp = threadIdx.x >> 5;
     float* s = s_dyn + warp * tile_smem_words<SIGMA>();
     const TilePolicy pol{l2_evict_last_policy(), l2_evict_first_policy()};
-    const long long chunk = (total_tiles + gridDim.x - 1) / gridDim.x;
-    const long long g0 = min64((long long)blockIdx.x * chunk, total_tiles);
-    const long long g1 = min64(g0 + chunk, total_tiles);
+    // CTAs take 32-tile sub-chunks round-robin (CTA b: sub-chunks b, b + G,
+    // ...), so every CTA samples the whole group: items whose tiles cost
+    // different amounts (banded rows gather from L1, power-law rows from L2)
+    // average out, where contiguous chunks left the slowest SM 26% above the
+    // mean. Warp w of the CTA takes tile w of the sub-chunk, so the 32 warps
+    // still work on 32 adjacent tiles. The fix-up is a separate pass over
+    // all tiles, so which CTA sums a tile does not matter.
+    const long long nsub = (total_tiles + kBatchWarps - 1) / kBatchWarps;
     int it = 0;
     long long lo = 0, hi = 0;
-    for (long long g = g0 + warp; g < g1; g += kBatchWarps) {
+    for (long long sc = blockIdx.x; sc < nsub; sc += gridDim.x) {
+        const long long g = sc * kBatchWarps + warp;
+        if (g >= total_tiles) continue;
         if (g < lo || g >= hi) {
             it = find_item(prefix, count, g);
             lo = __ldg(prefix + it);
