@@ -157,11 +157,14 @@ int mr_spmv_merbit(const mr_merbit_plan* plan, const mr_csr_view* A, const float
  * live in one file-scope device array sized for n_rows + nnz <= 2^24 merge
  * items (about 5.3 MB that every GPU which loads the library keeps until
  * exit); larger matrices return MR_ERR_UNSUPPORTED. The caller passes A, x
- * and y as for mr_spmv_merbit; each call rebuilds the plan into the array
- * and gives the same result as a planned call. The first call on a device
- * looks up the array's device address: make it before any stream capture.
- * All calls share the array, so calls that overlap on the GPU race:
- * order them on one stream. */
+ * and y as for mr_spmv_merbit. Each call checks the matrix as plan creation
+ * does and waits for that check on `stream` (a malformed rowptr or column
+ * index returns MR_ERR_INVALID_ARG before any gather), then rebuilds the
+ * plan into the array and gives bitwise the result of a planned call. The
+ * first call on a device looks up the array's device address and keeps it:
+ * make that first call before any stream capture, and make no call after
+ * cudaDeviceReset. All calls share the array, so calls that overlap on the
+ * GPU race: order them on one stream. */
 int mr_spmv_merbit_noalloc(const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
 
 /* ------------------------------------------------ batched SpMV ---- */

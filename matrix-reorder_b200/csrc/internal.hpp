@@ -78,6 +78,9 @@ int launch_permute_vector(int n, const int32_t* perm, const float* in, float* ou
 int launch_perm_invert(int n, const int32_t* perm, int32_t* inv, int* bad_flag, cudaStream_t st);
 int check_perm(const int32_t* perm, int n, int* valid, cudaStream_t st);
 int validate_csr(const mr_csr_view& A, int* ok, cudaStream_t st);
+// enqueues the checks of validate_csr; *bad_dev (zeroed by the caller) gets
+// 1 for a malformed rowptr, 2 for a column index outside [0, n_cols)
+int validate_csr_async(const mr_csr_view& A, int* bad_dev, cudaStream_t st);
 
 // device scan: out[i] = sum_{j<i} in[j], out[n] = total (n + 1 outputs)
 int exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t st);

@@ -14,18 +14,26 @@
 //    (n_rows + nnz <= 2^24) with SIGMA 14, about 5.3 MB that every GPU which
 //    loads the library keeps until the process exits; larger matrices get
 //    MR_ERR_UNSUPPORTED before any work is enqueued;
-//  * each call rebuilds the plan into the array (one extra kernel) and then
-//    runs the same persistent MERBIT kernel as mr_spmv_merbit, so results
-//    equal a planned call's;
+//  * each call first checks the matrix as plan creation does (rowptr
+//    starts at 0, never decreases and ends at nnz; every column index lies
+//    in [0, n_cols)), with the check's flag in the array, and waits for the
+//    answer on the caller's stream: a malformed matrix returns
+//    MR_ERR_INVALID_ARG before any gather is issued;
+//  * it then rebuilds the plan into the array (one extra kernel) and runs
+//    the same persistent MERBIT kernel as mr_spmv_merbit, so results are
+//    bitwise those of a planned call;
 //  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current); make that first call
-//    before any stream capture;
+//    (cudaGetSymbolAddress, with that device current) and keeps it for the
+//    process; make that first call before any stream capture. The kept
+//    address dies with the device's context: after cudaDeviceReset the
+//    entry point must not be called again in that process;
 //  * all calls share the array and it keeps the last call's contents, so
 //    calls whose work overlaps on the GPU (different streams, or threads
 //    without ordering) race: serialise them on one stream. Every call
 //    rewrites the plan and the carries before reading them, and clears the
-//    completion ticket of the persistent kernel (the one word that must
-//    start at zero) with cudaMemsetAsync, which allocates nothing.
+//    check flag and the completion ticket of the persistent kernel (the
+//    words that must start at zero) with cudaMemsetAsync, which allocates
+//    nothing.
 #include <mutex>
 
 #include "common.cuh"
@@ -45,6 +53,7 @@ constexpr size_t kOffTileY = kOffTileX + align256(4 * (kNoAllocMaxTiles + 1));
 constexpr size_t kOffDesc = kOffTileY + align256(4 * (kNoAllocMaxTiles + 1));
 constexpr size_t kOffCarry = kOffDesc + align256(4 * kNoAllocMaxLanes);
 constexpr size_t kOffTicket = kOffCarry + align256(4 * kNoAllocMaxTiles);
+constexpr size_t kOffFlag = kOffTicket + 128;  // validation flag, same 256-byte slot
 constexpr size_t kNoAllocBytes = kOffTicket + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -74,7 +83,7 @@ using namespace mr;
 
 extern "C" int mr_spmv_merbit_noalloc(const mr_csr_view* A, const float* x, float* y, void* stream)
 {
-    if (!A || A->n_rows < 0 || A->nnz < 0 || !A->rowptr) return MR_ERR_INVALID_ARG;
+    if (!A || A->n_rows < 0 || A->n_cols < 0 || A->nnz < 0 || !A->rowptr) return MR_ERR_INVALID_ARG;
     if (A->dtype != MR_F32 && A->dtype != MR_F16 && A->dtype != MR_BF16) return MR_ERR_UNSUPPORTED;
     if (A->n_rows > 0 && (!y || (A->nnz > 0 && (!x || !A->colidx || !A->vals)))) return MR_ERR_INVALID_ARG;
     const long long items = (long long)A->n_rows + A->nnz;
@@ -99,6 +108,18 @@ extern "C" int mr_spmv_merbit_noalloc(const mr_csr_view* A, const float* x, floa
     p.carry = reinterpret_cast<float*>(b + kOffCarry);
     p.ticket = reinterpret_cast<int*>(b + kOffTicket);
     cudaStream_t st = as_stream(stream);
+    // the matrix check, as at plan creation: its flag lives in the array and
+    // its answer comes back through a host word (no allocation either side)
+    int* flag = reinterpret_cast<int*>(b + kOffFlag);
+    MR_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), st));
+    MR_TRY(validate_csr_async(*A, flag, st));
+    int bad = 0;
+    MR_CUDA_TRY(cudaMemcpyAsync(&bad, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    MR_CUDA_TRY(cudaStreamSynchronize(st));
+    if (bad) {
+        note_error("mr_spmv_merbit_noalloc: malformed CSR (rowptr or a column index out of range)");
+        return MR_ERR_INVALID_ARG;
+    }
     MR_CUDA_TRY(cudaMemsetAsync(p.ticket, 0, sizeof(int), st));
     MR_TRY(launch_merbit_plan(A->rowptr, A->n_rows, (int)A->nnz, p.sigma, p.lane_num, p.tile_num, p.tile_x, p.tile_y,
                               p.lane_desc, st));

@@ -5,8 +5,9 @@
 # the stand-ins in oracle/ref_stubs/ (their libraries need boost, libnuma and
 # a network fetch). Nothing is copied out of the reference tree.
 set -euo pipefail
-REF=${MR_REFERENCE_DIR:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the reference checkout sits beside this repository unless MR_REFERENCE_DIR names it
+REF=${MR_REFERENCE_DIR:-$(dirname "$(dirname "$HERE")")/reference}
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/class.cu" ]; then
   echo "build_ref: reference sources not found at $REF; nothing built"

@@ -12,7 +12,8 @@ stores inputs and outputs in tests/golden/golden_host.npz:
   * rd_merbit_model::PredictSpeedup on feature vectors (include/model.cuh),
   * the band gate's decision counts (run_band_gate_scan,
     ridge/train.py:983-1026, imported from the reference checkout named by
-    MR_REFERENCE, default /root/reference) on seeded predicted / true
+    MR_REFERENCE, default the `reference` directory beside this
+    repository) on seeded predicted / true
     speedups for every BAND_GATE_PAIRS entry.
 
 Usage: python tests/golden/make_golden.py   (needs oracle/_ref built)
@@ -65,7 +66,8 @@ def main() -> None:
     out["predict_features"] = feats
     out["predict_ref"] = np.array([O.ref_predict(f) for f in feats])
     # band gate of the ridge trainer, run by the reference's own Python
-    ref = os.environ.get("MR_REFERENCE", "/root/reference")
+    # the reference checkout sits beside this repository unless MR_REFERENCE names it
+    ref = os.environ.get("MR_REFERENCE", os.path.join(os.path.dirname(REPO), "reference"))
     sys.path.insert(0, os.path.join(ref, "ridge"))
     import pandas as pd
     import train as T  # the reference's ridge/train.py
