@@ -183,8 +183,93 @@ def run_reference(args):
                                    "the reference has no CPU SpMV)"},
         "e2e": {"value": round(val, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    gk = reference_gpu_kernels(O, rp, ci, v, perm, brp, bci, bv, xp)
+    if gk:
+        line["reference_gpu_kernels"] = gk
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_gpu_kernels(O, rp, ci, v, perm, brp, bci, bv, xp):
+    """The reference's own GPU code of this path, compiled from its sources
+    into oracle/_ref and run on the same reordered matrix on this GPU:
+    Tile_Kernel + merbit_kernel<float,256,14> launched as GRAPH::spmv drives
+    them (400 launches, y/z float-atomic ping-pong, src/class.cu:1407-1430),
+    its plain-CSR path cuSPARSE CSR_ALG1 (src/class.cu:1359-1397),
+    sampled_hll_rd_block_kernel with locality_predict's settings (30,960
+    samples, p = 12, src/class.cu:1263-1311) and the relabel (Thrust gather
+    + GRAPH::sort(false), src/class.cu:2699-2705) of the original matrix by
+    the pGOrder permutation. None of this build's kernels runs here. Each
+    time is a mean over launches (CUDA events) or a median of synchronised
+    calls after one warm call."""
+    try:
+        import torch
+        if not torch.cuda.is_available() or O.ref() is None:
+            return None
+    except Exception:
+        return None
+    import ctypes as C
+    R = O.ref()
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    n, nnz = brp.size - 1, bci.size
+    b = spmv_bytes(n, nnz)
+    out = {"matrix": "the same pGOrder-reordered matrix as the headline"}
+    rpd, cid, vd, xd = d(brp), d(bci), d(bv), d(xp)
+    lane_num = (n + nnz + 13) // 14
+    tile_num = (lane_num + 31) // 32
+    tx = torch.zeros(tile_num + 1, dtype=torch.int32, device=dev)
+    ty = torch.zeros(tile_num + 1, dtype=torch.int32, device=dev)
+    ld = torch.zeros(lane_num, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = R.ref_tile_build(rpd.data_ptr(), n, nnz, tx.data_ptr(), ty.data_ptr(), ld.data_ptr())
+    t_tile = (time.perf_counter() - t0) * 1e3
+    y, z = torch.zeros(n, device=dev), torch.zeros(n, device=dev)
+    ms = C.c_float(0)
+    R.ref_merbit_spmv(rpd.data_ptr(), cid.data_ptr(), vd.data_ptr(), n, nnz, tx.data_ptr(), ty.data_ptr(),
+                      ld.data_ptr(), xd.data_ptr(), y.data_ptr(), z.data_ptr(), 20, C.byref(ms))
+    rc |= R.ref_merbit_spmv(rpd.data_ptr(), cid.data_ptr(), vd.data_ptr(), n, nnz, tx.data_ptr(), ty.data_ptr(),
+                            ld.data_ptr(), xd.data_ptr(), y.data_ptr(), z.data_ptr(), 400, C.byref(ms))
+    out["merbit_kernel_float_256_14"] = {"ms": round(ms.value, 5), "gbs": round(b / ms.value / 1e6, 1),
+                                         "tile_build_ms": round(t_tile, 3), "launches": 400}
+    R.ref_cusparse_spmv(rpd.data_ptr(), cid.data_ptr(), vd.data_ptr(), n, nnz, xd.data_ptr(), y.data_ptr(), 20,
+                        C.byref(ms))
+    rc |= R.ref_cusparse_spmv(rpd.data_ptr(), cid.data_ptr(), vd.data_ptr(), n, nnz, xd.data_ptr(), y.data_ptr(),
+                              400, C.byref(ms))
+    out["cusparse_csr_alg1"] = {"ms": round(ms.value, 5), "gbs": round(b / ms.value / 1e6, 1), "launches": 400}
+    del tx, ty, ld, y, z, rpd, vd, xd
+    samples, hp = 30960, 12
+    est = torch.empty(samples, dtype=torch.float32, device=dev)
+    st_ = torch.empty(samples, dtype=torch.int32, device=dev)
+    pos = torch.empty(samples, dtype=torch.int32, device=dev)
+    times = []
+    for _ in range(4):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc |= R.ref_hll_sampled(cid.data_ptr(), nnz, samples, 32, 246813579, 589824, 0, hp, est.data_ptr(),
+                                st_.data_ptr(), pos.data_ptr())
+        times.append((time.perf_counter() - t0) * 1e3)
+    out["sampled_hll_rd_block_kernel"] = {"ms": round(float(np.median(times[1:])), 2), "samples": samples,
+                                          "hll_p": hp}
+    del cid, est, st_, pos
+    rows = np.repeat(np.arange(rp.size - 1, dtype=np.int32), np.diff(rp))
+    pd = d(perm)
+    times = []
+    for _ in range(4):
+        row_ind, col_ind, vals = d(ci), d(rows), d(v)  # reference layout: row_ind = our column
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc |= R.ref_relabel_sort(n, nnz, row_ind.data_ptr(), col_ind.data_ptr(), vals.data_ptr(), pd.data_ptr())
+        times.append((time.perf_counter() - t0) * 1e3)
+        del row_ind, col_ind, vals
+    pb = 2 * (4 * (n + 1) + 8 * nnz) + 4 * n + 4 * nnz
+    mr = float(np.median(times[1:]))
+    out["relabel_gather_thrust_sort"] = {"ms": round(mr, 3), "gbs": round(pb / mr / 1e6, 1)}
+    out["cuda_status"] = int(rc)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
 
 
 def time_cpu_baseline(brp, bci, bv, xp, budget_s: float = 10.0):
@@ -202,6 +287,24 @@ def time_cpu_baseline(brp, bci, bv, xp, budget_s: float = 10.0):
             break
     dt = time.perf_counter() - t0
     return spmv_bytes(n, bci.size) * reps / dt / 1e9, used, reps
+
+
+def oracle_checks(rp, ci, v, x, perm, y_head, y_e2e, brp, bci, bv):
+    """The oracle (oracle/, test infrastructure) as this run's checker: FP64
+    CSR SpMV of the ORIGINAL matrix against the headline's result and the
+    e2e result, both un-permuted (y = P^T y'), and the device permutation
+    B = P A P^T against the oracle's restatement, bit for bit."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle as O
+    ref = O.spmv_f64(rp, ci, v, x)
+    nr = float(np.linalg.norm(ref))
+    out = {"rel_l2_vs_fp64_oracle": float(np.linalg.norm(y_head.astype(np.float64) - ref) / nr),
+           "e2e_rel_l2_vs_fp64_oracle": float(np.linalg.norm(y_e2e.astype(np.float64) - ref) / nr),
+           "tolerance": 1e-5}
+    orp, oci, ov = O.permute_csr(rp, ci, v, perm)
+    out["permuted_csr_bit_exact_vs_oracle"] = bool(np.array_equal(orp, brp) and np.array_equal(oci, bci) and
+                                                   np.array_equal(ov.view(np.uint32), bv.view(np.uint32)))
+    return out
 
 
 def reference_cpu_functions(rp, ci, bci, n):
@@ -259,7 +362,20 @@ def run_ours(args):
     t0 = time.perf_counter()
     M.permute_csr(A, perm_d, brp, bci, bv)
     torch.cuda.synchronize()
-    setup["permute_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    setup["permute_ms_first_call"] = round((time.perf_counter() - t0) * 1e3, 2)
+    # the first call of a process pays module loading and the scratch pool;
+    # the warm figure is the median of synchronised calls after it
+    p_times = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        M.permute_csr(A, perm_d, brp, bci, bv)
+        torch.cuda.synchronize()
+        p_times.append((time.perf_counter() - t0) * 1e3)
+    p_ms = float(np.median(p_times))
+    p_bytes = 2 * (4 * (n + 1) + 8 * nnz) + 4 * n + 4 * nnz
+    setup["permute_warm"] = {"ms_median": round(p_ms, 3), "ms_min": round(min(p_times), 3),
+                             "gbs": round(p_bytes / p_ms / 1e6, 1), "calls": len(p_times)}
     B = M.view(brp, bci, bv)
     xp = torch.empty_like(x_d)
     M.permute_vector(perm_d, x_d, xp, inverse=False)
@@ -346,6 +462,16 @@ def run_ours(args):
             lp_ms = (time.perf_counter() - t0) * 1e3
             details[f"rd_{name}"] = {"log2_counts": counts.tolist(), "reuses": valid, "exact_ms": round(rd_ms, 1),
                                      "predicted_speedup": round(sp, 4), "sampled_predict_ms": round(lp_ms, 2)}
+        # the sampled HLL kernel alone (30,960 samples, p = 12: the settings
+        # of the reference's locality_predict), median of synchronised calls
+        h_times = []
+        for _ in range(4):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            M.rd_hist_sampled(bci, samples=30960, hll_p=12)
+            torch.cuda.synchronize()
+            h_times.append((time.perf_counter() - t0) * 1e3)
+        details["rd_sampled_hll_ms"] = round(float(np.median(h_times[1:])), 2)
         details.update(laplace_companion(M, args, torch, timed, dev))
     inf = plan.info()
     details["hub_columns"] = inf.hub_columns
@@ -428,25 +554,27 @@ def run_ours(args):
     pcie = pcie_ceiling(torch, dev, n)
     served_check = float(torch.linalg.norm(y_ring[(k_e2e - 1) % 8].to(dev).double() - y_h.to(dev).double()) /
                          torch.linalg.norm(y_h.to(dev).double()))
-    # self-check of the e2e result: against the plain CSR kernel on the
-    # original (unreordered) matrix
-    y_csr = torch.empty_like(x_d)
-    M.spmv_csr(A, x_d, y_csr)
+    # the headline's last y' un-permuted (y = P^T y'), for the check against
+    # the FP64 SpMV of the original matrix below
+    y_head = torch.empty_like(x_d)
+    M.permute_vector(perm_d, yp, y_head, inverse=True)
     torch.cuda.synchronize()
-    got, ref = y_h.to(dev).double(), y_csr.double()  # y_h: the last e2e result
-    check = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+    y_head_h = y_head.cpu().numpy()
+    del y_head
 
     peak, peak_kind = peaks()
     achieved = bytes_step / (ms_step / 1e3) / 1e9
     persistent = args.block == 1024
+    # DRAM bytes of this exact kernel and matrix from its ncu capture (the
+    # profile names the command); None when no capture of this
+    # configuration exists
     traffic, traffic_src = traffic_from_profiles(
-        f"merbit_persistent_hub_rmat_s21.md" if persistent and hub_cache else "merbit_persistent_kernel_rmat_s21.md",
-        bytes_step)
+        f"merbit_persistent{'_hub' if hub_cache else ''}_rmat_s{args.scale}_sigma{args.sigma}.md"
+        if persistent else "", bytes_step)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_spmv": bytes_step,
-                "traffic_source": (f"profiles/{traffic_src}, R-MAT s21 capture scaled by algorithmic bytes"
-                                   if traffic_src else None),
+                "traffic_source": f"profiles/{traffic_src}" if traffic_src else None,
                 "kernels_timed": ("merbit_persistent_kernel (one launch per SpMV, fused fix-up)" if persistent
                                   else "merbit_spmv_kernel + merbit_fixup_kernel (two launches per SpMV)")}
     if "gather_ceiling_gbs" in details:
@@ -463,6 +591,10 @@ def run_ours(args):
         ref_fns = reference_cpu_functions(rp, ci, bci_h, n)
         if ref_fns:
             cpu["reference_functions"] = ref_fns
+        # the oracle as the checker of this run: FP64 SpMV of the original
+        # matrix against the headline's and the e2e path's un-permuted y, and
+        # the permuted CSR against the oracle's B = P A P^T bit for bit
+        cpu["checker"] = oracle_checks(rp, ci, v, x, perm, y_head_h, y_h.numpy(), brp_h, bci_h, bv_h)
 
     plan.close()
     if rank == 0:
@@ -483,18 +615,108 @@ def run_ours(args):
                     "copy_ceiling": dict(pcie, frac=round(pcie["bidir_ms_per_step"] / (ms_served / k_e2e), 4)),
                     "served_vs_sync_rel_l2": served_check,
                     "sync": {"value": round(e2e_sync_val, 1), "ms_per_step": round(ms_e2e / k_e2e, 4),
-                             "path": "mr_plain_requests (C-ABI, pinned host x/y, synchronised per step)",
-                             "rel_l2_vs_csr_orig": check}},
+                             "path": "mr_plain_requests (C-ABI, pinned host x/y, synchronised per step)"}},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": (1 if persistent else 2) * args.steps,
             "details": {**details, **setup},
         }
+        if cpu and "checker" in cpu:
+            line["details"]["rel_l2_vs_fp64_oracle"] = cpu["checker"]["rel_l2_vs_fp64_oracle"]
+            line["e2e"]["rel_l2_vs_fp64_oracle"] = cpu["checker"]["e2e_rel_l2_vs_fp64_oracle"]
+        if not args.quick and args.extras and ws == 1:
+            # the other BASELINE configurations, compact, after this
+            # workload's memory is released (results only; the headline
+            # above is what the line's value measures)
+            del A, B, rp_d, ci_d, v_d, x_d, perm_d, brp, bci, bv, xp, yp
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            line["details"]["configs"] = other_configs(args)
         print(json.dumps(line), flush=True)
     if dist:
         tdist.barrier()
         tdist.destroy_process_group()
     return 0
+
+
+def small_config(args):
+    """R-MAT scale 16, edge factor 16, seed 1 (65,536 rows, ~1M nonzeros):
+    host pGOrder (w = 5), the permutation on the GPU, MERBIT (the tuner's
+    pick, and the reference's SIGMA 14 / 256 threads) and plain CSR on the
+    reordered matrix, each result un-permuted and compared with an FP64 SpMV
+    of the original matrix (torch sparse CSR in float64 on the GPU). The
+    whole matrix (~8 MB) sits in L2, so its GB/s are not HBM figures."""
+    import torch
+    import mrb200 as M
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.from_numpy(a).to(dev)
+    rp, ci, v = M.gen_rmat(scale=16, edge_factor=16, seed=1)
+    n, nnz = rp.size - 1, ci.size
+    x = M.uniform(n, seed=1001)
+    n2o = M.pgorder(rp, ci, vsize=0, width=5)
+    perm = np.empty(n, np.int32)
+    perm[n2o] = np.arange(n, dtype=np.int32)
+    rp_d, ci_d, v_d, x_d, perm_d = d(rp), d(ci), d(v), d(x), d(perm)
+    A = M.view(rp_d, ci_d, v_d)
+    brp, bci, bv = torch.empty_like(rp_d), torch.empty_like(ci_d), torch.empty_like(v_d)
+    M.permute_csr(A, perm_d, brp, bci, bv)
+    B = M.view(brp, bci, bv)
+    xp, yp, y = torch.empty_like(x_d), torch.empty_like(x_d), torch.empty_like(x_d)
+    M.permute_vector(perm_d, x_d, xp, inverse=False)
+    ref = (torch.sparse_csr_tensor(rp_d.long(), ci_d.long(), v_d.double(), size=(n, n)) @
+           x_d.double().unsqueeze(1)).squeeze(1)
+    st = torch.cuda.current_stream()
+    b = spmv_bytes(n, nnz)
+
+    def timed(fn, steps=200):
+        for _ in range(10):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def err():
+        M.permute_vector(perm_d, yp, y, inverse=True)
+        torch.cuda.synchronize()
+        return float(torch.linalg.norm(y.double() - ref) / torch.linalg.norm(ref))
+
+    out = {"n_rows": n, "nnz": nnz, "pgorder_vsize": M.pgorder_width(n, nnz), "l2_resident": True}
+    sg, bl, fl, _ = M.autotune(B, xp, yp, reps=5)
+    for name, kw in (("merbit_tuned", dict(sigma=sg, block=bl, flags=fl)),
+                     ("merbit_sigma14_block256", dict(sigma=14, block=256, hub_cache=False))):
+        plan = M.MerbitPlan(B, **kw)
+        ms = timed(lambda: plan.spmv(xp, yp))
+        out[name] = {"ms": round(ms, 5), "gbs": round(b / ms / 1e6, 1), "rel_l2_vs_fp64": err()}
+        plan.close()
+    out["merbit_tuned"]["sigma_block_flags"] = [sg, bl, fl]
+    ms = timed(lambda: M.spmv_csr(B, xp, yp))
+    out["csr"] = {"ms": round(ms, 5), "gbs": round(b / ms / 1e6, 1), "rel_l2_vs_fp64": err()}
+    return out
+
+
+def other_configs(args):
+    """The other BASELINE configurations in one run, each compact: the small
+    R-MAT, the FP16/BF16 precision matrix, the 512-matrix batch and the
+    serving pool. A failure is recorded, not raised, so that the headline
+    line is always printed."""
+    import torch
+    out = {}
+    for name, fn in (("small_rmat_s16", small_config), ("precision_chung_lu_8m", precision_result),
+                     ("batch_512_graph", batch_result), ("serve_pool", serve_result)):
+        t0 = time.time()
+        try:
+            out[name] = fn(args)
+        except Exception as e:  # recorded in the line
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = round(time.time() - t0, 1)
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
 
 
 def laplace_companion(M, args, torch, timed, dev):
@@ -768,7 +990,7 @@ def run_csr(args):
     return 0
 
 
-def run_serve(args):
+def serve_result(args):
     """Serving workload: a resident pool of pGOrder-reordered FP16 matrices
     (rows log-uniform 4K..2M, degree 4..64, R-MAT / banded / Chung-Lu),
     Poisson requests, continuous batching; against the plain per-request FP32
@@ -884,11 +1106,15 @@ def run_serve(args):
                   "mean_nnz": int(np.mean([p["nnz"] for p in protos])),
                   "mean_rows": int(np.mean([p["n"] for p in protos]))},
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_serve(args):
+    print(json.dumps(serve_result(args)), flush=True)
     return 0
 
 
-def run_precision(args):
+def precision_result(args):
     """Precision workload: Chung-Lu power law (8M rows, exponent 2.1, mean
     degree 20, degrees clamped to [1, 200k]); values stored FP16 / BF16
     (rounded from the drawn values), x FP32, FP32 accumulation with the FP64
@@ -947,11 +1173,15 @@ def run_precision(args):
                        "max_degree": 200000, "order": "as generated"},
             "results": out, "setup": {"gen_s": round(gen_s, 1),
                                       "max_row_len": int(np.diff(rp).max())}}
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_precision(args):
+    print(json.dumps(precision_result(args)), flush=True)
     return 0
 
 
-def run_batch(args):
+def batch_result(args):
     """Batching workload: args.batch_count independent CSR matrices, rows
     log-uniform in [1K, 512K], each R-MAT (edge factor 8-32) or banded
     (bandwidth 3-65) by seeded choice, FP32 values / x uniform[-1,1], each
@@ -1040,7 +1270,11 @@ def run_batch(args):
             "setup": {"gen_reorder_s": round(gen_s, 1)}}
     batch.close()
     tuner.close()
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def run_batch(args):
+    print(json.dumps(batch_result(args)), flush=True)
     return 0
 
 
@@ -1062,6 +1296,8 @@ def main() -> int:
     ap.add_argument("--workload", choices=["spmv", "serve", "precision", "batch", "permute", "csr", "kernel"],
                     default="spmv")
     ap.add_argument("--no-hub", action="store_true", help="kernel: plan without the hub cache")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="spmv: skip the other configurations (small R-MAT, precision, batch, serving)")
     ap.add_argument("--cl-rows", type=int, default=8 * 1024 * 1024, help="precision: Chung-Lu rows")
     ap.add_argument("--pool", type=int, default=2000, help="serve: resident matrices")
     ap.add_argument("--protos", type=int, default=24, help="serve: distinct generated matrices in the pool")

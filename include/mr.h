@@ -408,9 +408,10 @@ int mr_order_degree(const mr_csr_view* A, int32_t* perm_old2new_dev, void* strea
 /* Degree-based grouping: class ceilf(log2(degree + 1.0)) decreasing, ids
  * increasing within a class: GRAPH::dbg (src/class.cu:1660-1760). */
 int mr_order_dbg(const mr_csr_view* A, int32_t* perm_old2new_dev, void* stream);
-/* A seeded uniform random permutation, standing in for
- * GRAPH::relabel_random (src/class.cu:1460-1491); not the same permutation
- * as the reference's thrust::shuffle for the same seed. */
+/* GRAPH::relabel_random (src/class.cu:1460-1491): the permutation the
+ * reference's thrust::shuffle of the identity draws with
+ * thrust::default_random_engine seeded with `seed` (the reference passes
+ * graph_id), bit for bit. */
 int mr_order_random(int32_t n, uint32_t seed, int32_t* perm_old2new_dev, void* stream);
 
 /* pGOrder on the GPU: the same permutation as mr_pgorder (bit for bit), one

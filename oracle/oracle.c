@@ -547,3 +547,47 @@ double orc_predict(const double* coef, double intercept, const double* r)
     for (int i = 0; i < 10; ++i) v += coef[i] * r[i];
     return exp(v);
 }
+
+/* ------------------------------------------------------- random order -- */
+
+/* minstd_rand (x <- 48271 x mod 2^31 - 1), Thrust's default_random_engine;
+ * seed(s) takes s mod m and replaces 0 by 1. */
+static uint32_t minstd_next(uint64_t* x)
+{
+    *x = (*x * 48271u) % 2147483647u;
+    return (uint32_t)*x;
+}
+
+void orc_order_random(int n, uint32_t seed, int32_t* perm)
+{
+    /* relabel_random seeds the engine with graph_id and shuffles the
+     * identity perm (src/class.cu:1467-1473); thrust::shuffle copies the
+     * input and writes out[j] = in[key_j], key_j the j-th value of the
+     * Feistel bijection below that is < n, taken in index order. */
+    uint64_t x = seed % 2147483647u;
+    if (x == 0) x = 1;
+    uint32_t key[24];
+    for (int i = 0; i < 24; ++i) key[i] = minstd_next(&x);
+    /* cipher width: 4 bits up to n = 16, else ceil(log2 n) */
+    uint32_t bits = 4;
+    if (n > 16) {
+        bits = 0;
+        for (uint64_t m = (uint64_t)n - 1; m; m >>= 1) ++bits;
+    }
+    const uint32_t lb = bits / 2, rb = bits - lb;
+    const uint64_t lmask = (1ull << lb) - 1, rmask = (1ull << rb) - 1;
+    const uint64_t span = 1ull << bits;
+    int64_t j = 0;
+    for (uint64_t v = 0; v < span; ++v) {
+        uint32_t a = (uint32_t)(v >> rb), b = (uint32_t)(v & rmask);
+        for (int r = 0; r < 24; ++r) {
+            const uint64_t p = 0xD2B74407B1CE6E93ull * (uint64_t)a;
+            const uint32_t hi = (uint32_t)(p >> 32);
+            const uint32_t lo = ((uint32_t)p << (rb - lb)) | (b >> lb);
+            a = (uint32_t)(((hi ^ key[r]) ^ b) & lmask);
+            b = (uint32_t)(lo & rmask);
+        }
+        const uint64_t k = ((uint64_t)a << rb) | b;
+        if (k < (uint64_t)n) perm[j++] = (int32_t)k;
+    }
+}

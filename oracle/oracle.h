@@ -70,6 +70,14 @@ int orc_get_width(int nrow, int nnz);
 /* exp(intercept + sum coef_i * r_i) (include/model.cuh:84-95). */
 double orc_predict(const double* coef10, double intercept, const double* r10);
 
+/* GRAPH::relabel_random (src/class.cu:1460-1491): perm_old2new = the
+ * identity shuffled by thrust::shuffle with thrust::default_random_engine
+ * seeded with graph_id. The algorithm is Thrust's (CCCL bundled with CUDA
+ * 12.9, thrust/system/detail/generic/shuffle.inl): a 24-round Feistel
+ * bijection over the next power of two >= n, compacted to [0, n) in index
+ * order. */
+void orc_order_random(int n, uint32_t seed, int32_t* perm_old2new);
+
 #ifdef __cplusplus
 }
 #endif

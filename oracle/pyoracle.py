@@ -48,6 +48,7 @@ def orc():
         _sig(L.orc_pgorder, None, i32, vp, vp, i32, i32, vp)
         _sig(L.orc_get_width, C.c_int, i32, i32)
         _sig(L.orc_predict, C.c_double, vp, C.c_double, vp)
+        _sig(L.orc_order_random, None, i32, u32, vp)
         _orc = L
     return _orc
 
@@ -75,6 +76,7 @@ def ref():
         _sig(L.ref_relabel_sort, C.c_int, i32, i32, vp, vp, vp, vp)
         _sig(L.ref_gorder4_full, C.c_int, i32, i32, vp, vp, vp, i32, i32, vp)
         _sig(L.ref_relabel_order, C.c_int, i32, i32, i32, vp, vp, vp, i32, vp)
+        _sig(L.ref_shuffle_host, C.c_int, i32, u32, vp)
         _sig(L.ref_cusparse_spmv, C.c_int, vp, vp, vp, i32, i32, vp, vp, i32, C.POINTER(C.c_float))
         _ref = L
     return _ref
@@ -235,6 +237,23 @@ def order_degree(rowptr, colidx):
     perm = np.empty(n, np.int32)
     perm[order] = np.arange(n, dtype=np.int32)
     return perm
+
+
+def order_random(n: int, seed: int) -> np.ndarray:
+    """GRAPH::relabel_random (src/class.cu:1460-1491): thrust::shuffle of the
+    identity with default_random_engine(graph_id) (oracle.c restatement of
+    Thrust's Feistel-bijection shuffle); perm[old] = new."""
+    perm = np.empty(n, np.int32)
+    orc().orc_order_random(n, seed, _p(perm))
+    return perm
+
+
+def ref_shuffle(n: int, seed: int) -> np.ndarray:
+    """Thrust's own shuffle (host backend) of the identity, seeded as
+    relabel_random seeds it (oracle/_ref)."""
+    out = np.empty(n, np.int32)
+    ref().ref_shuffle_host(n, seed, _p(out))
+    return out
 
 
 def order_dbg(rowptr, colidx):

@@ -8,7 +8,7 @@
  * and kernels so that tests can compare the product against them.
  *
  * Host-only entry points (run in any container): ref_get_width,
- * ref_rd_hist_exact, ref_pgorder_host, ref_predict.
+ * ref_rd_hist_exact, ref_pgorder_host, ref_predict, ref_shuffle_host.
  * Device entry points (need a GPU): ref_tile_build, ref_merbit_spmv,
  * ref_hll_sampled, ref_relabel_sort, ref_gorder4_full, ref_relabel_order, ref_cusparse_spmv.
  *
@@ -267,6 +267,22 @@ int ref_cusparse_spmv(const int* d_rowptr, const int* d_colidx, const float* d_v
     cusparseDestroyDnVec(Y);
     cusparseDestroy(h);
     return (int)cudaDeviceSynchronize();
+}
+
+/* The permutation GRAPH::relabel_random draws (src/class.cu:1467-1473):
+ * thrust::shuffle of the identity with thrust::default_random_engine seeded
+ * with graph_id, here run by Thrust's host backend (the same generic
+ * algorithm as the device call) so that fixtures can be made without a GPU.
+ * out[old] = new. */
+int ref_shuffle_host(int n, unsigned int seed, int* out)
+{
+    thrust::host_vector<int> v(n);
+    thrust::sequence(thrust::host, v.begin(), v.end());
+    thrust::default_random_engine rng;
+    rng.seed(seed);
+    thrust::shuffle(thrust::host, v.begin(), v.end(), rng);
+    for (int i = 0; i < n; ++i) out[i] = v[i];
+    return 0;
 }
 
 } /* extern "C" */

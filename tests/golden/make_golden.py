@@ -34,8 +34,24 @@ import pyoracle as O  # noqa: E402
 LOG2_EDGES = [1 << k for k in range(0, 13)]
 
 
+RANDOM_CASES = [(1, 0), (16, 3), (17, 1), (1000, 0), (4096, 42), (30011, 7)]
+
+
+def random_orders() -> None:
+    """tests/golden/golden_random.npz: the permutation GRAPH::relabel_random
+    draws (src/class.cu:1467-1473), from Thrust's own shuffle run through the
+    reference build's host entry point, for (n, graph_id) pairs."""
+    assert O.ref_available(), "build oracle/_ref first (oracle/build_ref.sh)"
+    out = {"cases": np.array(RANDOM_CASES, np.int64)}
+    for n, seed in RANDOM_CASES:
+        out[f"perm_{n}_{seed}"] = O.ref_shuffle(n, seed)
+    np.savez_compressed(os.path.join(HERE, "golden_random.npz"), **out)
+    print("wrote", os.path.join(HERE, "golden_random.npz"))
+
+
 def main() -> None:
     assert O.ref_available(), "build oracle/_ref first (oracle/build_ref.sh)"
+    random_orders()
     out = {}
     cases = {
         "rmat12": M.gen_rmat(scale=12, edge_factor=8, seed=3)[:2],

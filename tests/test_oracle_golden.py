@@ -1,8 +1,9 @@
 """Pins the CPU oracle and the product's host code to the reference.
 
-Fixtures in tests/golden/golden_host.npz come from the reference's own code
-(tests/golden/make_golden.py). When oracle/_ref is built in this container the
-same functions are also compared live on larger inputs.
+Fixtures in tests/golden/golden_host.npz come from the reference's own code,
+those in golden_random.npz from Thrust's shuffle that the reference's
+relabel_random calls (tests/golden/make_golden.py). When oracle/_ref is built
+in this container the same functions are also compared live on larger inputs.
 """
 import os
 
@@ -89,3 +90,23 @@ class TestLiveReference:
         for _ in range(20):
             f = rng.dirichlet(np.ones(10))
             assert M.predict_speedup(f) == O.ref_predict(f)
+
+
+R_FIX = np.load(os.path.join(GOLDEN, "golden_random.npz"))
+
+
+@pytest.mark.parametrize("n,seed", [tuple(int(a) for a in c) for c in R_FIX["cases"]])
+def test_random_order_oracle_matches_thrust_shuffle(O, n, seed):
+    """GRAPH::relabel_random's permutation (thrust::shuffle, seeded with
+    graph_id): the oracle's restatement against fixtures from Thrust's own
+    implementation (tests/golden/make_golden.py)."""
+    got = O.order_random(n, seed)
+    assert np.array_equal(got, R_FIX[f"perm_{n}_{seed}"])
+    assert np.array_equal(np.sort(got), np.arange(n))
+
+
+def test_random_order_oracle_matches_thrust_live(O):
+    if not O.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    for n, seed in ((100003, 0), (1 << 20, 12345), (3, 9)):
+        assert np.array_equal(O.order_random(n, seed), O.ref_shuffle(n, seed)), (n, seed)

@@ -1,7 +1,8 @@
 """Comparator permutation producers on the GPU (degree, DBG, random): the
 degree and DBG orders equal the oracle's restatement of GRAPH::relabel_degree
 / GRAPH::dbg and the reference's own functions run on the B200; the random
-order is a seeded bijection (not the reference's thrust::shuffle stream)."""
+order equals the oracle's restatement of GRAPH::relabel_random and the
+reference's own relabel_random (thrust::shuffle) run on the B200."""
 import numpy as np
 import pytest
 
@@ -75,6 +76,47 @@ def test_random_order_is_a_seeded_bijection(M):
     # no long identity runs: a shuffle, not a near-identity map
     assert np.mean(pa == np.arange(n)) < 1e-3
     assert M.check_perm(a)
+
+
+@pytest.mark.parametrize("n", [1, 16, 17, 4096, 100003, 1 << 20, 4194304])
+def test_random_order_matches_oracle(M, O, n):
+    import torch
+    for seed in (0, 1, 7):
+        p = torch.empty(n, dtype=torch.int32, device="cuda")
+        M.order_random(n, seed, p)
+        torch.cuda.synchronize()
+        assert np.array_equal(p.cpu().numpy(), O.order_random(n, seed)), (n, seed)
+
+
+def test_random_order_matches_reference_relabel_random(M, O, mats):
+    """GRAPH::relabel_random itself (thrust::shuffle on the device, seeded
+    with graph_id) on the B200: the same permutation and, applied through
+    mr_permute_csr, the same relabelled matrix."""
+    R = O.ref()
+    if R is None:
+        pytest.skip("reference build (oracle/_ref) not present")
+    import torch
+    for name, gid in (("rmat14", 0), ("chung_lu", 7), ("random", 123)):
+        rp, ci, v = mats[name]
+        n = rp.size - 1
+        rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(rp))
+        row_ind, col_ind, vals = _dev(ci.copy()), _dev(rows), _dev(v.copy())  # reference layout
+        ref = np.empty(n, np.int32)
+        assert R.ref_relabel_order(2, n, int(ci.size), row_ind.data_ptr(), col_ind.data_ptr(), vals.data_ptr(), gid,
+                                   ref.ctypes.data) == 0
+        p = torch.empty(n, dtype=torch.int32, device="cuda")
+        M.order_random(n, gid, p)
+        A = M.view(_dev(rp), _dev(ci), _dev(v))
+        orp = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        oci = torch.empty(ci.size, dtype=torch.int32, device="cuda")
+        ov = torch.empty(ci.size, dtype=torch.float32, device="cuda")
+        M.permute_csr(A, p, orp, oci, ov)
+        torch.cuda.synchronize()
+        assert np.array_equal(p.cpu().numpy(), ref), name
+        g_rows = np.repeat(np.arange(n, dtype=np.int32), np.diff(orp.cpu().numpy()))
+        assert np.array_equal(col_ind.cpu().numpy(), g_rows), name
+        assert np.array_equal(row_ind.cpu().numpy(), oci.cpu().numpy()), name
+        assert np.array_equal(vals.cpu().numpy().view(np.uint32), ov.cpu().numpy().view(np.uint32)), name
 
 
 def test_invalid_input_rejected(M):
