@@ -189,16 +189,32 @@ __device__ __forceinline__ void merbit_tile(const MerbitOperand<V, SIGMA>& m, co
 
     float rows[SIGMA];  // finished row sums, indexed by the item that ends them
     float cur = 0.f;
+    // every lane of a tile before the last holds SIGMA items: that walk
+    // needs no per-item range test
+    if ((int64_t)(tile + 1) * 32 * SIGMA <= m.items) {
 #pragma unroll
-    for (int i = 0; i < SIGMA; ++i) {
-        rows[i] = 0.f;
-        if (i < lane_items) {
+        for (int i = 0; i < SIGMA; ++i) {
+            rows[i] = 0.f;
             if ((flags >> i) & 1u) {
                 rows[i] = cur;
                 cur = 0.f;
             } else {
                 cur += s[xi];
                 ++xi;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < SIGMA; ++i) {
+            rows[i] = 0.f;
+            if (i < lane_items) {
+                if ((flags >> i) & 1u) {
+                    rows[i] = cur;
+                    cur = 0.f;
+                } else {
+                    cur += s[xi];
+                    ++xi;
+                }
             }
         }
     }
