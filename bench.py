@@ -1088,7 +1088,11 @@ def serve_result(args):
                    "host_vectors": "page-locked (both paths)", "hbm_budget_gb": round(budget / 2**30, 1)},
         "saturation": {**{k: round(sat[k], 1) for k in ("req_per_s", "p50_us", "p99_us", "mean_batch")},
                        "completed": sat["completed"],
-                       "gbs": round(sat["req_per_s"] * mean_b16 / 1e9, 1)},
+                       "gbs": round(sat["req_per_s"] * mean_b16 / 1e9, 1),
+                       # device time per request of each stage, summed over the
+                       # batches (copies and kernels of different batches overlap)
+                       "us_per_request": {k: round(sat[k] * 1e3 / max(sat["completed"], 1), 2)
+                                          for k in ("h2d_ms", "compute_ms", "d2h_ms", "launch_ms")}},
         "poisson": {"rate": args.rate, **{k: round(pois[k], 1) for k in ("req_per_s", "p50_us", "p99_us",
                                                                           "mean_batch")},
                     "completed": pois["completed"], "evictions": pois["evictions"]},

@@ -142,16 +142,7 @@ int mr_merbit_plan_create_ex(const mr_csr_view* A, int sigma, int block, int fla
     const size_t desc_bytes = sigma < 15 ? 4 : 8;
     cudaStream_t st = as_stream(stream);
     auto fail = [&](int code) {
-        cudaFree(p.tile_x);
-        cudaFree(p.tile_y);
-        cudaFree(p.lane_desc);
-        cudaFree(p.carry);
-        cudaFree(p.ticket);
-        cudaFree(p.colh);
-        cudaFree(p.hub_cols);
-        cudaFree(p.chunk_start);
-        cudaFree(p.boundary_run);
-        cudaFree(p.boundary_flag);
+        free_plan_buffers(p);
         delete h;
         return code;
     };
@@ -189,16 +180,7 @@ int mr_merbit_plan_destroy(mr_merbit_plan* h)
     cudaGetDevice(&dev);
     if (dev != h->p.device) cudaSetDevice(h->p.device);
     cudaDeviceSynchronize();
-    cudaFree(h->p.tile_x);
-    cudaFree(h->p.tile_y);
-    cudaFree(h->p.lane_desc);
-    cudaFree(h->p.carry);
-    cudaFree(h->p.ticket);
-    cudaFree(h->p.colh);
-    cudaFree(h->p.hub_cols);
-    cudaFree(h->p.chunk_start);
-    cudaFree(h->p.boundary_run);
-    cudaFree(h->p.boundary_flag);
+    free_plan_buffers(h->p);
     if (dev != h->p.device) cudaSetDevice(dev);
     delete h;
     return MR_OK;

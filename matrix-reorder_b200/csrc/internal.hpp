@@ -56,6 +56,8 @@ bool merbit_sigma_supported(int sigma);
 int build_hub_cache(MerbitPlan& p, const mr_csr_view& A, cudaStream_t st);
 // cost-balanced CTA chunks of a persistent-kernel plan (after the hub cache)
 int build_chunk_bounds(MerbitPlan& p, const int* colidx, cudaStream_t st);
+// frees every device buffer a plan owns
+void free_plan_buffers(MerbitPlan& p);
 // CTAs of the persistent kernel for a plan of tile_num tiles on this device
 int persistent_grid(int tile_num);
 // largest number of hub slots that fit beside the SIGMA staging buffers

@@ -659,6 +659,20 @@ int build_hub_cache(MerbitPlan& p, const mr_csr_view& A, cudaStream_t st)
     return MR_OK;
 }
 
+void free_plan_buffers(MerbitPlan& p)
+{
+    cudaFree(p.tile_x);
+    cudaFree(p.tile_y);
+    cudaFree(p.lane_desc);
+    cudaFree(p.carry);
+    cudaFree(p.ticket);
+    cudaFree(p.colh);
+    cudaFree(p.hub_cols);
+    cudaFree(p.chunk_start);
+    cudaFree(p.boundary_run);
+    cudaFree(p.boundary_flag);
+}
+
 int persistent_grid(int tile_num)
 {
     return std::max(1, std::min(sm_count(), (tile_num + kPersistWarps - 1) / kPersistWarps));

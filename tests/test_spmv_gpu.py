@@ -122,11 +122,28 @@ def test_merbit_spmv_matches_fp64(M, O, cases, sigma):
 
 @pytest.mark.parametrize("block", [128, 256, 512, 1024])
 def test_merbit_block_sizes(M, O, cases, block):
-    rp, ci, v = cases["rmat13"]
-    x = M.uniform(rp.size - 1, seed=5)
-    plan, y, _ = _plan_and_spmv(M, rp, ci, v, x, block=block)
-    assert _rel_l2(y, O.spmv_f64(rp, ci, v, x)) <= REL_L2_F32
-    plan.close()
+    """Every form (grid kernels of 4 / 8 / 16 warps with the separate fix-up
+    kernel, and the persistent kernel with its fused fix-up) against FP64,
+    and bit for bit against the persistent form, on every edge case (huge
+    rows give carry runs that span many CTAs); repeated launches of one plan
+    give the same bits (the persistent kernel's arrival counters and ticket
+    reset themselves)."""
+    import torch
+    for name, (rp, ci, v) in cases.items():
+        ncols = max(rp.size - 1, int(ci.max(initial=0)) + 1)
+        x = M.uniform(ncols, seed=5)
+        for sigma in (7, 14, 20):
+            plan, y, _ = _plan_and_spmv(M, rp, ci, v, x, sigma=sigma, block=block)
+            ref_plan, y_ref, _ = _plan_and_spmv(M, rp, ci, v, x, sigma=sigma, block=1024)
+            assert _rel_l2(y, O.spmv_f64(rp, ci, v, x)) <= REL_L2_F32, (name, sigma)
+            assert np.array_equal(y.view(np.int32), y_ref.view(np.int32)), (name, sigma)
+            y2 = torch.full((rp.size - 1,), float("nan"), device="cuda")
+            for _ in range(2):
+                plan.spmv(_dev(x), y2)
+            torch.cuda.synchronize()
+            assert np.array_equal(y2.cpu().numpy().view(np.int32), y.view(np.int32)), (name, sigma)
+            plan.close()
+            ref_plan.close()
 
 
 @pytest.mark.parametrize("sigma", [7, 14, 32])
