@@ -221,14 +221,15 @@ int mr_tuner_stats(mr_tuner* tuner, int32_t* buckets, int32_t* tuned);
  * planned on first use, within hbm_budget_bytes, evicting the least
  * recently used idle matrices. A scheduler thread batches the requests that
  * arrive within window_us of the first pending one (at most max_batch) and
- * keeps up to `lanes` batches in flight on separate streams. Each request's
+ * keeps up to `lanes` batches in flight, pipelined (copies in, kernels,
+ * copies out, each stage in launch order on its own stream). Each request's
  * result is bitwise the same alone or in any batch. */
 typedef struct mr_server mr_server;
 typedef struct mr_server_config {
     int64_t hbm_budget_bytes; /* device bytes for resident matrices; 0 = half the free memory */
     int32_t window_us;        /* batching window (default 200) */
     int32_t max_batch;        /* requests per batch (default 64) */
-    int32_t lanes;            /* batches in flight, one stream each (default 3) */
+    int32_t lanes;            /* batches in flight, one buffer set each (default 3) */
     int32_t sigma;            /* MERBIT sigma of resident plans (default 14) */
 } mr_server_config;
 typedef struct mr_server_stats {

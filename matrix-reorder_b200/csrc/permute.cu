@@ -182,23 +182,47 @@ int check_perm(const int32_t* perm, int n, int* valid, cudaStream_t st)
     return MR_OK;
 }
 
-__global__ void permute_vector_kernel(int n, const int32_t* __restrict__ perm, const float* __restrict__ in,
-                                      float* __restrict__ out, int inverse)
+// A block covers kPvPer * 256 consecutive elements, thread t the elements
+// t, t + 256, ...: the thread loads its kPvPer permutation entries, then its
+// kPvPer inputs, then stores, so that kPvPer independent loads are in flight
+// per thread at each step (the random side, the gather of the inverse or the
+// scatter of the forward permutation, is the latency-bound one).
+constexpr int kPvPer = 4;
+
+__global__ void __launch_bounds__(256) permute_vector_kernel(int n, const int32_t* __restrict__ perm,
+                                                             const float* __restrict__ in, float* __restrict__ out,
+                                                             int inverse)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int p = perm[i];
-        if (p < 0 || p >= n) continue;
+    const int64_t base = (int64_t)blockIdx.x * (256 * kPvPer) + threadIdx.x;
+    int p[kPvPer];
+    float v[kPvPer];
+#pragma unroll
+    for (int e = 0; e < kPvPer; ++e) {
+        const int64_t i = base + 256 * e;
+        p[e] = i < n ? __ldg(perm + i) : -1;
+        if (p[e] >= n) p[e] = -1;  // not a permutation entry: skipped
+    }
+#pragma unroll
+    for (int e = 0; e < kPvPer; ++e) {
+        const int64_t i = base + 256 * e;
+        v[e] = p[e] < 0 ? 0.f : (inverse ? __ldg(in + p[e]) : __ldg(in + i));
+    }
+#pragma unroll
+    for (int e = 0; e < kPvPer; ++e) {
+        const int64_t i = base + 256 * e;
+        if (p[e] < 0) continue;
         if (inverse)
-            out[i] = in[p];
+            out[i] = v[e];
         else
-            out[p] = in[i];
+            out[p[e]] = v[e];
     }
 }
 
 int launch_permute_vector(int n, const int32_t* perm, const float* in, float* out, int inverse, cudaStream_t st)
 {
     if (n <= 0) return MR_OK;
-    permute_vector_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, perm, in, out, inverse);
+    const int grid = (int)(((int64_t)n + 256 * kPvPer - 1) / (256 * kPvPer));
+    permute_vector_kernel<<<grid, 256, 0, st>>>(n, perm, in, out, inverse);
     MR_CUDA_TRY(cudaGetLastError());
     return MR_OK;
 }

@@ -9,24 +9,30 @@
 //    y = P^T y'. A matrix becomes resident on first use: upload + MERBIT plan
 //    into stream-ordered device memory, admitted against an HBM budget, the
 //    least recently used idle matrices evicted first.
-//  * Streams: each lane copies on its own stream; the kernels of all batches
-//    run in launch order on one compute stream (event-joined to the lanes),
-//    so copies of some batches overlap the kernels of others while the
-//    persistent batch kernels never contend with each other for the SMs.
+//  * Streams: a three-stage pipeline in launch order: the host-to-device
+//    copies of every batch on one stream, the kernels on a second, the
+//    device-to-host copies on a third (event-joined per batch). The copies
+//    of batch k + 1 overlap the kernels of batch k, the persistent batch
+//    kernels never contend with each other for the SMs, and each batch's
+//    copies run alone on their copy direction, so a batch's inputs arrive
+//    as early as the link allows instead of sharing it with the batches
+//    queued behind it.
 //  * Batching: a scheduler thread waits `window_us` after the first pending
 //    request (or until max_batch are pending), takes the pending requests in
 //    arrival order, admits their matrices and launches the batch on a free
-//    lane (stream); up to `lanes` batches are in flight, so requests that
+//    lane (a set of buffers and events); up to `lanes` batches are in flight, so requests that
 //    arrive while others are on the GPU form the next batch and overlap on
 //    the device (continuous batching). A batch is: the H2D copies of its x
 //    vectors, one batched permutation, the batched MERBIT kernels (one per
 //    (sigma, dtype) group), one batched un-permutation, the D2H copies. The
 //    scheduler issues a batch without holding the server lock, so submits
 //    are never blocked behind the launch.
-//  * Host vectors: x and y in page-locked memory (cudaHostAlloc, or
-//    cudaHostRegister over the whole vector) are copied by the copy engines
-//    straight from / into the caller's buffer; other host memory goes
-//    through the lane's pinned staging area with a host memcpy.
+//  * Host vectors: x and y of 256 KB and more in page-locked memory
+//    (cudaHostAlloc, or cudaHostRegister over the whole vector) are copied
+//    by the copy engines straight from / into the caller's buffer; smaller
+//    ones, and host memory that is not page-locked, go through the lane's
+//    pinned staging area with a host memcpy, all of a batch's in one DMA
+//    each way.
 //  * Completion: a thread waits on each lane's event in launch order, copies
 //    staged results to the callers' y, records latency (submit -> result in
 //    y).
@@ -67,23 +73,29 @@ struct PermOp {
 
 // Batched permutation of every item's vector, as a gather on both sides so
 // that the writes are coalesced: inverse == 0 gives x'[j] = x[n2o[j]]
-// (x' = P x), inverse != 0 gives y[i] = y'[perm[i]] (y = P^T y'). Each
-// thread walks a contiguous range of the arena and looks its item up again
-// only when it crosses into the next one.
-__global__ void batch_permute_kernel(const PermOp* __restrict__ ops, const long long* __restrict__ prefix, int count,
-                                     long long total, const float* __restrict__ in, float* __restrict__ out,
-                                     int inverse)
+// (x' = P x), inverse != 0 gives y[i] = y'[perm[i]] (y = P^T y'). A block
+// covers kPermPer * 256 consecutive elements of the batch arena, thread t
+// the elements t, t + 256, ...: every thread first loads its kPermPer
+// indices, then issues its kPermPer gathers, then stores, so that each
+// thread has kPermPer independent loads in flight per step. A thread looks
+// its item up (binary search in the prefix) for its first element and again
+// only when one of its elements crosses into the next item.
+constexpr int kPermPer = 8;
+
+__global__ void __launch_bounds__(256)
+    batch_permute_kernel(const PermOp* __restrict__ ops, const long long* __restrict__ prefix, int count,
+                         long long total, const float* __restrict__ in, float* __restrict__ out, int inverse)
 {
-    const long long nthreads = (long long)gridDim.x * blockDim.x;
-    const long long per = (total + nthreads - 1) / nthreads;
-    // consecutive threads take consecutive elements of a block-sized stripe
-    const long long stripe = (long long)blockDim.x;
-    const long long b0 = (long long)blockIdx.x * blockDim.x * per;
-    const long long b1 = b0 + (long long)blockDim.x * per < total ? b0 + (long long)blockDim.x * per : total;
+    const long long base = (long long)blockIdx.x * (256 * kPermPer) + threadIdx.x;
     int it = -1;
     long long lo = 0, hi = 0;
     const int32_t* idx = nullptr;
-    for (long long g = b0 + threadIdx.x; g < b1; g += stripe) {
+    long long src[kPermPer];
+#pragma unroll
+    for (int e = 0; e < kPermPer; ++e) {
+        const long long g = base + 256ll * e;
+        src[e] = -1;
+        if (g >= total) continue;
         if (g < lo || g >= hi) {
             int a = 0, b = count - 1;  // largest item whose offset is <= g
             while (a < b) {
@@ -98,7 +110,15 @@ __global__ void batch_permute_kernel(const PermOp* __restrict__ ops, const long 
             hi = it + 1 < count ? __ldg(prefix + it + 1) : total;
             idx = inverse ? ops[it].perm : ops[it].n2o;
         }
-        out[g] = idx ? __ldg(in + lo + __ldg(idx + (g - lo))) : __ldg(in + g);
+        src[e] = idx ? lo + __ldg(idx + (g - lo)) : g;
+    }
+    float v[kPermPer];
+#pragma unroll
+    for (int e = 0; e < kPermPer; ++e) v[e] = src[e] >= 0 ? __ldg(in + src[e]) : 0.f;
+#pragma unroll
+    for (int e = 0; e < kPermPer; ++e) {
+        const long long g = base + 256ll * e;
+        if (g < total) out[g] = v[e];
     }
 }
 
@@ -113,6 +133,14 @@ bool host_pinned(const void* p)
     return a.type == cudaMemoryTypeHost;
 }
 
+// Vectors below this size move through the lane's page-locked staging
+// buffers (a host memcpy into one contiguous region, then one DMA each way
+// for all of them): every DMA has a fixed cost, and with both directions
+// busy, a batch's small copies cut each direction's throughput by about a
+// third (32 copies of log-uniform 16 KB .. 8 MB: 31 GB/s per direction;
+// staging those below 256 KB: 39 GB/s; one copy per direction: 47 GB/s).
+constexpr size_t kStageBelowBytes = 256 << 10;
+
 struct Request {
     uint64_t ticket = 0;
     int id = 0;
@@ -124,6 +152,12 @@ struct Request {
     int status = MR_OK;
     bool done = false;
 };
+
+// the request's x and y move through the staging buffers
+bool item_staged(const Request& r, int32_t n)
+{
+    return !r.x_pinned || !r.y_pinned || sizeof(float) * (size_t)n < kStageBelowBytes;
+}
 
 struct Matrix {
     int32_t n = 0;
@@ -189,8 +223,8 @@ struct DevVec {
     }
 };
 
+// the buffers and events of one batch in flight
 struct Lane {
-    cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     cudaEvent_t ev_start = nullptr, ev_h2d = nullptr, ev_kern = nullptr;  // stage boundaries (timing)
     PinnedVec<float> hx, hy;
@@ -200,6 +234,7 @@ struct Lane {
     std::vector<long long> off;
     std::vector<int> mats;
     std::vector<Matrix*> mp;  // the batch's matrices, read by launch_batch without the lock
+    int n_staged = 0;         // items 0 .. n_staged-1 move through hx / hy
     bool busy = false;
 };
 
@@ -220,7 +255,9 @@ struct mr_server {
     bool stop = false;
     std::thread sched, compl_;
     cudaStream_t admit_st = nullptr;
-    cudaStream_t compute_st = nullptr;  // the batches' kernels, in launch order (copies stay on the lanes)
+    cudaStream_t h2d_st = nullptr;      // the batches' host-to-device copies, in launch order
+    cudaStream_t compute_st = nullptr;  // the batches' kernels, in launch order
+    cudaStream_t d2h_st = nullptr;      // the batches' device-to-host copies, in launch order
     int* d_flag = nullptr;  // device word for launch_perm_invert
     int device = 0;
     // stats
@@ -338,24 +375,50 @@ bool make_room(mr_server* s, size_t need, const std::vector<int>& keep)
 int launch_batch(mr_server* s, Lane& L)
 {
     const int count = (int)L.reqs.size();
-    L.off.assign((size_t)count + 1, 0);
-    for (int i = 0; i < count; ++i) L.off[(size_t)i + 1] = L.off[(size_t)i] + L.mp[(size_t)i]->n;
-    const long long total = L.off[(size_t)count];
-    bool staged = false;
-    for (const Request* r : L.reqs) staged = staged || !r->x_pinned || !r->y_pinned;
-    if (staged) {
-        MR_TRY(L.hx.reserve((size_t)total + 1));
-        MR_TRY(L.hy.reserve((size_t)total + 1));
+    // staged items (small vectors, or a vector not page-locked) go first, so
+    // that they form one contiguous region of the arena and of the staging
+    // buffers: one DMA each way for all of them
+    {
+        std::vector<int> order((size_t)count);
+        for (int i = 0; i < count; ++i) order[(size_t)i] = i;
+        auto staged_item = [&](int i) { return item_staged(*L.reqs[(size_t)i], L.mp[(size_t)i]->n); };
+        std::stable_partition(order.begin(), order.end(), staged_item);
+        std::vector<Request*> reqs((size_t)count);
+        std::vector<int> mats((size_t)count);
+        std::vector<Matrix*> mp((size_t)count);
+        for (int i = 0; i < count; ++i) {
+            const int o = order[(size_t)i];
+            reqs[(size_t)i] = L.reqs[(size_t)o];
+            mats[(size_t)i] = L.mats[(size_t)o];
+            mp[(size_t)i] = L.mp[(size_t)o];
+        }
+        L.reqs.swap(reqs);
+        L.mats.swap(mats);
+        L.mp.swap(mp);
     }
-    for (int i = 0; i < count; ++i)
-        if (!L.reqs[(size_t)i]->x_pinned)
-            std::memcpy(L.hx.p + L.off[(size_t)i], L.reqs[(size_t)i]->x,
-                        sizeof(float) * (size_t)(L.off[(size_t)i + 1] - L.off[(size_t)i]));
+    L.off.assign((size_t)count + 1, 0);
+    L.n_staged = 0;
+    for (int i = 0; i < count; ++i) {
+        L.off[(size_t)i + 1] = L.off[(size_t)i] + L.mp[(size_t)i]->n;
+        if (item_staged(*L.reqs[(size_t)i], L.mp[(size_t)i]->n)) L.n_staged = i + 1;
+    }
+    const long long total = L.off[(size_t)count];
+    const long long staged_elems = L.off[(size_t)L.n_staged];
+    if (staged_elems > 0) {
+        MR_TRY(L.hx.reserve((size_t)staged_elems));
+        MR_TRY(L.hy.reserve((size_t)staged_elems));
+    }
+    for (int i = 0; i < L.n_staged; ++i)
+        std::memcpy(L.hx.p + L.off[(size_t)i], L.reqs[(size_t)i]->x,
+                    sizeof(float) * (size_t)(L.off[(size_t)i + 1] - L.off[(size_t)i]));
     const size_t vbytes = sizeof(float) * (size_t)(total + 1);
-    MR_TRY(L.dx.reserve(vbytes, L.st));
-    MR_TRY(L.dxp.reserve(vbytes, L.st));
-    MR_TRY(L.dyp.reserve(vbytes, L.st));
-    MR_TRY(L.dy.reserve(vbytes, L.st));
+    // a lane's buffers are (re)allocated in the order of the copy stream
+    // that first writes them; the lane is idle (its last batch completed)
+    cudaStream_t st = s->h2d_st;
+    MR_TRY(L.dx.reserve(vbytes, st));
+    MR_TRY(L.dxp.reserve(vbytes, st));
+    MR_TRY(L.dyp.reserve(vbytes, st));
+    MR_TRY(L.dy.reserve(vbytes, st));
     // group the items by (sigma, dtype): one batched kernel per group
     std::map<std::pair<int, int>, std::vector<int>> groups;
     long long carry_total = 0;
@@ -366,7 +429,7 @@ int launch_batch(mr_server* s, Lane& L)
         carry_off[(size_t)i] = carry_total;
         carry_total += std::max(m.plan.tile_num, 1);
     }
-    MR_TRY(L.carry.reserve(sizeof(float) * (size_t)carry_total, L.st));
+    MR_TRY(L.carry.reserve(sizeof(float) * (size_t)carry_total, st));
     // the small tables (batch operands per group, tile prefixes, permutation
     // operands) live in one pinned block per lane and go over in one copy:
     // a pageable source could make the copy wait for the lane's stream
@@ -378,7 +441,7 @@ int launch_batch(mr_server* s, Lane& L)
     const size_t at_pprefix = at_pops + a256(sizeof(PermOp) * (size_t)count);
     const size_t meta_bytes = at_pprefix + sizeof(long long) * ((size_t)count + 1);
     MR_TRY(L.meta_h.reserve(meta_bytes));
-    MR_TRY(L.meta_d.reserve(meta_bytes, L.st));
+    MR_TRY(L.meta_d.reserve(meta_bytes, st));
     unsigned char* mh = L.meta_h.p;
     unsigned char* md = static_cast<unsigned char*>(L.meta_d.p);
     long long* prefix_host = reinterpret_cast<long long*>(mh + at_prefix);
@@ -418,21 +481,18 @@ int launch_batch(mr_server* s, Lane& L)
         pops[(size_t)i] = PermOp{m.d_perm, m.d_n2o, L.off[(size_t)i], m.n};
     }
     std::memcpy(mh + at_pprefix, L.off.data(), sizeof(long long) * ((size_t)count + 1));
-    cudaStream_t st = L.st;
     MR_CUDA_TRY(cudaEventRecord(L.ev_start, st));
     MR_CUDA_TRY(cudaMemcpyAsync(md, mh, meta_bytes, cudaMemcpyHostToDevice, st));
-    for (int i = 0; i < count; ++i) {
-        const Request* r = L.reqs[(size_t)i];
+    if (staged_elems > 0)
+        MR_CUDA_TRY(cudaMemcpyAsync(dx, L.hx.p, sizeof(float) * (size_t)staged_elems, cudaMemcpyHostToDevice, st));
+    for (int i = L.n_staged; i < count; ++i) {
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
-        MR_CUDA_TRY(cudaMemcpyAsync(dx + o, r->x_pinned ? r->x : L.hx.p + o, nb, cudaMemcpyHostToDevice, st));
+        MR_CUDA_TRY(cudaMemcpyAsync(dx + o, L.reqs[(size_t)i]->x, nb, cudaMemcpyHostToDevice, st));
     }
     MR_CUDA_TRY(cudaEventRecord(L.ev_h2d, st));
-    // kernels of every lane run in launch order on one stream: concurrent
-    // persistent batch kernels of several lanes only contend for the SMs
-    cudaStream_t lane_st = st;
     st = s->compute_st;
     MR_CUDA_TRY(cudaStreamWaitEvent(st, L.ev_h2d, 0));
-    const int pgrid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, (long long)sm_count() * 4));
+    const int pgrid = (int)std::max<long long>(1, (total + 256 * kPermPer - 1) / (256 * kPermPer));
     const PermOp* d_pops = reinterpret_cast<const PermOp*>(md + at_pops);
     const long long* d_pprefix = reinterpret_cast<const long long*>(md + at_pprefix);
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dx, dxp, 0);
@@ -444,12 +504,13 @@ int launch_batch(mr_server* s, Lane& L)
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
     MR_CUDA_TRY(cudaGetLastError());
     MR_CUDA_TRY(cudaEventRecord(L.ev_kern, st));
-    st = lane_st;
+    st = s->d2h_st;
     MR_CUDA_TRY(cudaStreamWaitEvent(st, L.ev_kern, 0));
-    for (int i = 0; i < count; ++i) {
-        const Request* r = L.reqs[(size_t)i];
+    if (staged_elems > 0)
+        MR_CUDA_TRY(cudaMemcpyAsync(L.hy.p, dy, sizeof(float) * (size_t)staged_elems, cudaMemcpyDeviceToHost, st));
+    for (int i = L.n_staged; i < count; ++i) {
         const size_t o = (size_t)L.off[(size_t)i], nb = sizeof(float) * ((size_t)L.off[(size_t)i + 1] - o);
-        MR_CUDA_TRY(cudaMemcpyAsync(r->y_pinned ? r->y : L.hy.p + o, dy + o, nb, cudaMemcpyDeviceToHost, st));
+        MR_CUDA_TRY(cudaMemcpyAsync(L.reqs[(size_t)i]->y, dy + o, nb, cudaMemcpyDeviceToHost, st));
     }
     MR_CUDA_TRY(cudaEventRecord(L.done, st));
     return MR_OK;
@@ -577,9 +638,8 @@ void completion_loop(mr_server* s)
         }
         // results to the callers' buffers
         if (e == cudaSuccess)
-            for (size_t i = 0; i < L.reqs.size(); ++i)
-                if (!L.reqs[i]->y_pinned)
-                    std::memcpy(L.reqs[i]->y, L.hy.p + L.off[i], sizeof(float) * (size_t)(L.off[i + 1] - L.off[i]));
+            for (size_t i = 0; i < (size_t)L.n_staged; ++i)
+                std::memcpy(L.reqs[i]->y, L.hy.p + L.off[i], sizeof(float) * (size_t)(L.off[i + 1] - L.off[i]));
         lk.lock();
         s->t_h2d_ms += t_h2d;
         s->t_kern_ms += t_kern;
@@ -640,12 +700,13 @@ int mr_server_create(const mr_server_config* cfg, mr_server** out)
     }
     s->lanes.resize((size_t)s->cfg.lanes);
     bool ok = cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->h2d_st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&s->compute_st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->d2h_st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&s->d_flag, sizeof(int)) == cudaSuccess &&
               cudaMemset(s->d_flag, 0, sizeof(int)) == cudaSuccess;
     for (auto& L : s->lanes)
-        ok = ok && cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreate(&L.done) == cudaSuccess && cudaEventCreate(&L.ev_start) == cudaSuccess &&
+        ok = ok && cudaEventCreate(&L.done) == cudaSuccess && cudaEventCreate(&L.ev_start) == cudaSuccess &&
              cudaEventCreate(&L.ev_h2d) == cudaSuccess && cudaEventCreate(&L.ev_kern) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -848,14 +909,14 @@ int mr_server_destroy(mr_server* s)
             if (d->p) cudaFreeAsync(d->p, s->admit_st);
         for (cudaEvent_t ev : {L.done, L.ev_start, L.ev_h2d, L.ev_kern})
             if (ev) cudaEventDestroy(ev);
-        if (L.st) cudaStreamDestroy(L.st);
     }
     if (s->admit_st) {
         cudaStreamSynchronize(s->admit_st);
         cudaStreamDestroy(s->admit_st);
     }
     if (s->d_flag) cudaFree(s->d_flag);
-    if (s->compute_st) cudaStreamDestroy(s->compute_st);
+    for (cudaStream_t st : {s->h2d_st, s->compute_st, s->d2h_st})
+        if (st) cudaStreamDestroy(st);
     for (auto& kv : s->reqs) delete kv.second;
     for (Request* r : s->pending)
         if (s->reqs.find(r->ticket) == s->reqs.end()) delete r;
