@@ -582,6 +582,16 @@ def run_ours(args):
     if "gather_ceiling_gbs" in details:
         roofline["gather_ceiling"] = {"achieved": details["gather_ceiling_gbs"], "unit": "GB/s",
                                       "frac_of_ceiling": round(achieved / details["gather_ceiling_gbs"], 4)}
+    if "cusparse_orig_gbs" in details:
+        # against the reference's plain-CSR path (cuSPARSE CSR_ALG1) on the
+        # same arrays: the plan-free CSR kernel, and the planned MERBIT path
+        # built from the same CSR arrays (the drop-in for the reference's csr
+        # method, which has a setup stage of its own)
+        details["vs_cusparse"] = {
+            "csr_plan_free": {"orig": round(details["csr_orig_gbs"] / details["cusparse_orig_gbs"], 3),
+                              "reordered": round(details["csr_reordered_gbs"] / details["cusparse_reordered_gbs"], 3)},
+            "merbit_planned": {"orig": round(details["merbit_orig_gbs"] / details["cusparse_orig_gbs"], 3),
+                               "reordered": round(value / ws / details["cusparse_reordered_gbs"], 3)}}
 
     cpu = None
     if rank == 0 and not args.quick and args.cpu_budget > 0:

@@ -24,9 +24,10 @@
 //    bitwise those of a planned call;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress, with that device current) and keeps it for the
-//    process; make that first call before any stream capture. The kept
-//    address dies with the device's context: after cudaDeviceReset the
-//    entry point must not be called again in that process;
+//    process. The kept address dies with the device's context: after
+//    cudaDeviceReset the entry point must not be called again in that
+//    process. (The wait for the matrix check makes every call
+//    synchronise its stream, so no call can be captured into a graph);
 //  * all calls share the array and it keeps the last call's contents, so
 //    calls whose work overlaps on the GPU (different streams, or threads
 //    without ordering) race: serialise them on one stream. Every call
