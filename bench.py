@@ -52,6 +52,13 @@ def peaks():
         return HBM_FALLBACK_GBS, "fallback"
 
 
+def workload_config(args, n: int, nnz: int) -> dict:
+    """The headline workload, the same in both arms (the method is in the
+    line's "plan")."""
+    return {"workload": f"rmat_s{args.scale}_ef{args.edge_factor} pGOrder-reordered FP32 SpMV", "n_rows": n,
+            "nnz": nnz, "seed": args.seed}
+
+
 def spmv_bytes(n: int, nnz: int, val_bytes: int = 4) -> int:
     return 4 * (n + 1) + nnz * (4 + val_bytes) + 4 * n + 4 * n
 
@@ -176,8 +183,8 @@ def run_reference(args):
         "metric": "spmv_hbm_gbs", "value": round(val, 2), "unit": "GB/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"rmat_s{args.scale}_ef{args.edge_factor} pGOrder-reordered CSR SpMV", "n_rows": n,
-                   "nnz": nnz, "seed": args.seed},
+        "config": workload_config(args, n, nnz),
+        "plan": {"method": "FP32 CSR SpMV on the host cores (OpenMP)"},
         "cpu_baseline": {"value": round(val, 2), "unit": "GB/s", "cores": used, "kind": "port",
                          "sample": f"{args.steps} full FP32 CSR SpMVs of the reordered matrix (OpenMP restatement; "
                                    "the reference has no CPU SpMV)"},
@@ -389,6 +396,12 @@ def run_ours(args):
         setup["autotune_s"] = round(time.perf_counter() - t0, 2)
     else:
         flags = 0
+        if not args.quick:
+            # what the tuner would pick on this matrix (reported, not used)
+            t0 = time.perf_counter()
+            sg, bl, fl, _ = M.autotune(B, xp, yp, reps=5)
+            setup["autotune_pick"] = {"sigma": sg, "block": bl, "hub_cache": (fl & M.PLAN_NO_HUB_CACHE) == 0,
+                                      "s": round(time.perf_counter() - t0, 2)}
     hub_cache = (flags & M.PLAN_NO_HUB_CACHE) == 0
     # pGOrder on the GPU (same permutation as the host ordering above)
     try:
@@ -530,7 +543,8 @@ def run_ours(args):
     # requests overlap across lanes (copies of one with the SpMV of others).
     # Time = first submit to last result, from the server's own clock.
     brp_h, bci_h, bv_h = brp.cpu().numpy(), bci.cpu().numpy(), bv.cpu().numpy()
-    srv = M.Server(window_us=20, max_batch=2, lanes=8, sigma=args.sigma)
+    srv = M.Server(window_us=20, max_batch=args.e2e_max_batch, lanes=8, sigma=args.sigma,
+                   hub_cache=not args.e2e_no_hub)
     sid = srv.add_matrix(brp_h, bci_h, bv_h, perm)
     y_ring = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(8)]
     y_ring_np = [t.numpy() for t in y_ring]
@@ -614,16 +628,17 @@ def run_ours(args):
             "metric": "spmv_hbm_gbs", "value": round(value, 1), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_step, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"rmat_s{args.scale}_ef{args.edge_factor} pGOrder-reordered MERBIT FP32 SpMV",
-                       "n_rows": n, "nnz": nnz, "seed": args.seed, "sigma": args.sigma, "block": args.block,
-                       "hub_cache": bool(hub_cache), "tuned": bool(args.tune),
-                       "parallelism": f"replicas x{ws}",
-                       "l2": "inputs larger than L2 (matrix stream ~%d MB per step)" % (bytes_step // 2**20)},
+            "config": workload_config(args, n, nnz),
+            "plan": {"method": "MERBIT", "sigma": args.sigma, "block": args.block, "hub_cache": bool(hub_cache),
+                     "tuned": bool(args.tune), "parallelism": f"replicas x{ws}",
+                     "l2": "inputs larger than L2 (matrix stream ~%d MB per step)" % (bytes_step // 2**20)},
             "roofline": roofline,
             "e2e": {"value": round(e2e_val, 1), "unit": "GB/s", "h2d_bytes_per_step": 4 * n,
                     "d2h_bytes_per_step": 4 * n, "steps": k_e2e, "ms_per_step": round(ms_served / k_e2e, 4),
                     "path": "mr_server (C-ABI request API, pinned host x/y, requests overlapped on 8 lanes, "
-                            "batched MERBIT without hub cache)",
+                            f"{args.e2e_max_batch} per batch, " +
+                            ("batched MERBIT without hub cache)" if args.e2e_no_hub
+                             else "the matrix's persistent MERBIT plan with hub cache)"),
                     "copy_ceiling": dict(pcie, frac=round(pcie["bidir_ms_per_step"] / (ms_served / k_e2e), 4)),
                     "served_vs_sync_rel_l2": served_check,
                     "sync": {"value": round(e2e_sync_val, 1), "ms_per_step": round(ms_e2e / k_e2e, 4),
@@ -1317,9 +1332,16 @@ def main() -> int:
     ap.add_argument("--sigma", type=int, default=14)
     ap.add_argument("--block", type=int, default=1024)
     ap.add_argument("--e2e-steps", type=int, default=400)
+    ap.add_argument("--e2e-max-batch", type=int, default=2, help="e2e: requests per server batch")
+    ap.add_argument("--e2e-no-hub", action="store_true",
+                    help="e2e: the server's batched kernel instead of the persistent hub-cache plan")
     ap.add_argument("--cpu-budget", type=float, default=8.0, help="seconds of CPU-baseline timing")
     ap.add_argument("--quick", action="store_true", help="skip companion numbers and CPU baseline")
-    ap.add_argument("--no-tune", dest="tune", action="store_false", help="use --sigma/--block instead of the autotuner")
+    ap.add_argument("--tune", dest="tune", action="store_true",
+                    help="let the autotuner pick sigma / threads / hub cache for the headline (default: --sigma "
+                         "--block with the hub cache, the tuner's usual pick at R-MAT s22; the tuner times "
+                         "candidates, so under a profiler it can pick another plan)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="use --sigma/--block (the default)")
     ap.add_argument("--workload", choices=["spmv", "serve", "precision", "batch", "permute", "csr", "kernel"],
                     default="spmv")
     ap.add_argument("--no-hub", action="store_true", help="kernel: plan without the hub cache")

@@ -231,6 +231,9 @@ typedef struct mr_server_config {
     int32_t max_batch;        /* requests per batch (default 64) */
     int32_t lanes;            /* batches in flight, one buffer set each (default 3) */
     int32_t sigma;            /* MERBIT sigma of resident plans (default 14) */
+    int32_t hub_cache;        /* nonzero: each resident matrix gets the single-matrix persistent plan
+                                 (1024 threads, hub cache; about 4 more bytes of HBM per nonzero) and
+                                 runs in its own launch instead of the batched kernel (default 0) */
 } mr_server_config;
 typedef struct mr_server_stats {
     int64_t submitted, completed, rejected, batches, admissions, evictions;

@@ -24,7 +24,9 @@
 //    arrive while others are on the GPU form the next batch and overlap on
 //    the device (continuous batching). A batch is: the H2D copies of its x
 //    vectors, one batched permutation, the batched MERBIT kernels (one per
-//    (sigma, dtype) group), one batched un-permutation, the D2H copies. The
+//    (sigma, dtype) group; with `hub_cache`, each matrix's own persistent
+//    plan with the hub cache instead, one launch per item), one batched
+//    un-permutation, the D2H copies. The
 //    scheduler issues a batch without holding the server lock, so submits
 //    are never blocked behind the launch.
 //  * Host vectors: x and y of 256 KB and more in page-locked memory
@@ -167,6 +169,8 @@ struct Matrix {
     const int32_t* h_colidx = nullptr;
     const void* h_vals = nullptr;
     const int32_t* h_perm = nullptr;
+    int sigma = 14;           // MERBIT sigma of its plan
+    bool persistent = false;  // single-matrix persistent plan with the hub cache, own launch
     // device state while resident
     bool resident = false;
     int refs = 0;
@@ -280,10 +284,15 @@ namespace {
 size_t matrix_bytes(const Matrix& m)
 {
     const int64_t items = (int64_t)m.n + m.nnz;
-    const int64_t lanes = (items + 13) / 14;
+    const int64_t lanes = (items + m.sigma - 1) / m.sigma;
     const int64_t tiles = (lanes + 31) / 32;
-    return sizeof(int32_t) * ((size_t)m.n + 1) + (sizeof(int32_t) + dtype_size(m.dtype)) * (size_t)m.nnz +
-           (m.h_perm ? 2 * sizeof(int32_t) * (size_t)m.n : 0) + 4 * (size_t)lanes + 8 * (size_t)(tiles + 1) + 1024;
+    size_t b = sizeof(int32_t) * ((size_t)m.n + 1) + (sizeof(int32_t) + dtype_size(m.dtype)) * (size_t)m.nnz +
+               (m.h_perm ? 2 * sizeof(int32_t) * (size_t)m.n : 0) + (m.sigma < 15 ? 4 : 8) * (size_t)lanes +
+               8 * (size_t)(tiles + 1) + 1024;
+    // the persistent plan adds the hub-remapped colidx, per-tile carries, the
+    // hub column list and the per-CTA chunk tables (a bound)
+    if (m.persistent) b += sizeof(int32_t) * (size_t)m.nnz + sizeof(float) * (size_t)tiles + (1u << 20);
+    return b;
 }
 
 void free_resident(Matrix& m, cudaStream_t st)
@@ -296,6 +305,12 @@ void free_resident(Matrix& m, cudaStream_t st)
     cudaFreeAsync(m.plan.tile_x, st);
     cudaFreeAsync(m.plan.tile_y, st);
     cudaFreeAsync(m.plan.lane_desc, st);
+    // the persistent plan's own buffers (cudaMalloc'd by the plan builders);
+    // the matrix is idle, its last batch retired
+    for (void* q : {(void*)m.plan.carry, (void*)m.plan.ticket, (void*)m.plan.colh, (void*)m.plan.hub_cols,
+                    (void*)m.plan.chunk_start, (void*)m.plan.boundary_run, (void*)m.plan.boundary_flag})
+        if (q) cudaFree(q);
+    m.plan = MerbitPlan();
     m.d_rowptr = m.d_colidx = m.d_perm = m.d_n2o = nullptr;
     m.d_vals = nullptr;
     m.plan.tile_x = m.plan.tile_y = nullptr;
@@ -310,8 +325,9 @@ int make_resident(mr_server* s, Matrix& m)
     const size_t vb = dtype_size(m.dtype);
     auto alloc = [&](void** p, size_t b) { return cudaMallocAsync(p, std::max<size_t>(b, 16), st) == cudaSuccess; };
     m.plan = MerbitPlan();
-    m.plan.sigma = s->cfg.sigma;
+    m.plan.sigma = m.sigma;
     m.plan.block = 256;
+    cudaGetDevice(&m.plan.device);
     m.plan.n_rows = m.n;
     m.plan.nnz = m.nnz;
     const int64_t items = (int64_t)m.n + m.nnz;
@@ -342,6 +358,22 @@ int make_resident(mr_server* s, Matrix& m)
     int rc = rc0 != MR_OK ? rc0
                           : launch_merbit_plan(m.d_rowptr, m.n, (int)m.nnz, m.plan.sigma, m.plan.lane_num,
                                                m.plan.tile_num, m.plan.tile_x, m.plan.tile_y, m.plan.lane_desc, st);
+    if (rc == MR_OK && m.persistent) {
+        // the single-matrix persistent plan: carries, completion ticket, hub
+        // cache and cost-balanced CTA chunks, as mr_merbit_plan_create builds
+        m.plan.block = 1024;
+        if (cudaMalloc(&m.plan.carry, sizeof(float) * (size_t)std::max(m.plan.tile_num, 1)) != cudaSuccess ||
+            cudaMalloc(&m.plan.ticket, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = MR_ERR_NOMEM;
+        } else if (cudaMemsetAsync(m.plan.ticket, 0, sizeof(int), st) != cudaSuccess) {
+            rc = MR_ERR_CUDA;
+        } else {
+            const mr_csr_view A{m.n, m.n, m.nnz, m.d_rowptr, m.d_colidx, m.d_vals, m.dtype};
+            rc = build_hub_cache(m.plan, A, st);
+            if (rc == MR_OK) rc = build_chunk_bounds(m.plan, m.d_colidx, st);
+        }
+    }
     if (rc == MR_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = MR_ERR_CUDA;
     if (rc != MR_OK) {
         free_resident(m, st);
@@ -419,13 +451,18 @@ int launch_batch(mr_server* s, Lane& L)
     MR_TRY(L.dxp.reserve(vbytes, st));
     MR_TRY(L.dyp.reserve(vbytes, st));
     MR_TRY(L.dy.reserve(vbytes, st));
-    // group the items by (sigma, dtype): one batched kernel per group
+    // group the items by (sigma, dtype): one batched kernel per group; items
+    // with a persistent plan run alone, one launch each
     std::map<std::pair<int, int>, std::vector<int>> groups;
+    std::vector<int> solo;
     long long carry_total = 0;
     std::vector<long long> carry_off((size_t)count);
     for (int i = 0; i < count; ++i) {
         const Matrix& m = *L.mp[(size_t)i];
-        groups[{m.plan.sigma, m.dtype}].push_back(i);
+        if (m.persistent)
+            solo.push_back(i);
+        else
+            groups[{m.plan.sigma, m.dtype}].push_back(i);
         carry_off[(size_t)i] = carry_total;
         carry_total += std::max(m.plan.tile_num, 1);
     }
@@ -501,6 +538,12 @@ int launch_batch(mr_server* s, Lane& L)
         MR_TRY(batch_launch_ops(g.dtype, g.sigma, md + g.ops_at,
                                 reinterpret_cast<const long long*>(md + at_prefix) + g.prefix_at, g.count, g.tiles,
                                 st));
+    // one plan's launches never overlap: they are ordered on this stream
+    for (int i : solo) {
+        const Matrix& m = *L.mp[(size_t)i];
+        MR_TRY(launch_merbit_spmv(m.plan, m.d_colidx, m.d_vals, m.dtype, dxp + L.off[(size_t)i],
+                                  dyp + L.off[(size_t)i], m.plan.carry, st));
+    }
     batch_permute_kernel<<<pgrid, 256, 0, st>>>(d_pops, d_pprefix, count, total, dyp, dy, 1);
     MR_CUDA_TRY(cudaGetLastError());
     MR_CUDA_TRY(cudaEventRecord(L.ev_kern, st));
@@ -759,6 +802,8 @@ int mr_server_add_matrix(mr_server* s, int32_t n, int64_t nnz, const int32_t* ro
     m.h_colidx = colidx;
     m.h_vals = vals;
     m.h_perm = perm_old2new;
+    m.sigma = s->cfg.sigma;
+    m.persistent = s->cfg.hub_cache != 0;
     auto pm = std::unique_ptr<Matrix>(new (std::nothrow) Matrix(m));
     if (!pm) return MR_ERR_NOMEM;
     s->mats.push_back(std::move(pm));

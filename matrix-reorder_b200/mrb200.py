@@ -632,7 +632,7 @@ class Tuner:
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("window_us", C.c_int32), ("max_batch", C.c_int32),
-                ("lanes", C.c_int32), ("sigma", C.c_int32)]
+                ("lanes", C.c_int32), ("sigma", C.c_int32), ("hub_cache", C.c_int32)]
 
 
 class ServerStats(C.Structure):
@@ -671,10 +671,10 @@ class Server:
     as long as the server may read or write them."""
 
     def __init__(self, hbm_budget_bytes: int = 0, window_us: int = 200, max_batch: int = 64, lanes: int = 3,
-                 sigma: int = 14):
+                 sigma: int = 14, hub_cache: bool = False):
         L = lib()
         _server_sigs(L)
-        cfg = ServerConfig(hbm_budget_bytes, window_us, max_batch, lanes, sigma)
+        cfg = ServerConfig(hbm_budget_bytes, window_us, max_batch, lanes, sigma, 1 if hub_cache else 0)
         h = C.c_void_p()
         check(L.mr_server_create(C.byref(cfg), C.byref(h)), "mr_server_create")
         self.h = h

@@ -168,3 +168,70 @@ def test_loadgen_poisson(M, pool):
     st = srv.stats()
     assert st["h2d_ms"] == 0 and st["compute_ms"] == 0 and st["launch_ms"] == 0
     srv.close()
+
+
+def _big_pool(M):
+    """Matrices whose vectors straddle the staging threshold (256 KB = 65,536
+    floats): R-MAT scale 12 and 15 (staged) and 17 (copied directly when the
+    vectors are page-locked)."""
+    import pyoracle as O
+    mats = []
+    for i, sc in enumerate((12, 17, 15)):
+        rp, ci, v = M.gen_rmat(scale=sc, edge_factor=12, seed=30 + i)
+        n2o = M.pgorder(rp, ci, 0, 5)
+        perm = np.empty(rp.size - 1, np.int32)
+        perm[n2o] = np.arange(rp.size - 1, dtype=np.int32)
+        mats.append(dict(orig=(rp, ci, v), reordered=O.permute_csr(rp, ci, v, perm), perm=perm))
+    return mats
+
+
+@pytest.mark.parametrize("hub_cache", [False, True])
+def test_staged_and_direct_copies_in_one_batch(M, O, hub_cache):
+    """Page-locked vectors above the staging threshold go by their own DMA,
+    smaller ones through the staging buffer, in one batch: each result is
+    bitwise the one the request gets alone, and within 1e-5 of FP64. With
+    the hub cache each matrix runs its own persistent plan."""
+    import torch
+    mats = _big_pool(M)
+    srv = M.Server(window_us=2000, max_batch=16, lanes=2, sigma=20, hub_cache=hub_cache)
+    ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in mats]
+    jobs = []
+    for k in range(9):
+        j = k % 3
+        n = mats[j]["perm"].size
+        x = torch.from_numpy(M.uniform(n, seed=200 + k)).pin_memory()
+        y = torch.full((n,), float("nan")).pin_memory()
+        jobs.append((j, x, y))
+    alone = []
+    for j, x, y in jobs:
+        ya = np.full(x.numel(), np.nan, np.float32)
+        assert srv.wait(srv.submit(ids[j], x.numpy(), ya))[0] == M.MR_OK
+        alone.append(ya)
+    tickets = [srv.submit(ids[j], x.numpy(), y.numpy()) for j, x, y in jobs]
+    for t in tickets:
+        assert srv.wait(t)[0] == M.MR_OK
+    assert srv.stats()["batches"] < 9 + 9  # the burst was batched
+    for (j, x, y), ya in zip(jobs, alone):
+        assert np.array_equal(ya.view(np.int32), y.numpy().view(np.int32))
+        rp, ci, v = mats[j]["orig"]
+        assert _rel(y.numpy(), O.spmv_f64(rp, ci, v, x.numpy())) <= 1e-5
+    srv.close()
+
+
+def test_hub_cache_server_matches_batched_server(M, pool):
+    """The same requests through a server of batched plans and one of
+    persistent hub-cache plans: the same SpMV up to summation order."""
+    outs = []
+    for hub in (False, True):
+        srv = M.Server(window_us=200, lanes=3, hub_cache=hub)
+        ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
+        ys = []
+        for j, m in enumerate(pool):
+            x = M.uniform(m["perm"].size, seed=300 + j)
+            y = np.full(x.size, np.nan, np.float32)
+            assert srv.wait(srv.submit(ids[j], x, y))[0] == M.MR_OK
+            ys.append(y)
+        srv.close()
+        outs.append(ys)
+    for a, b in zip(*outs):
+        assert _rel(b, a.astype(np.float64)) <= 1e-6
