@@ -548,8 +548,13 @@ def run_ours(args):
     sid = srv.add_matrix(brp_h, bci_h, bv_h, perm)
     y_ring = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(8)]
     y_ring_np = [t.numpy() for t in y_ring]
-    for j in range(8):  # admission (upload + plan) and warm-up
-        srv.submit(sid, xh_np, y_ring_np[j])
+    # admission (upload + plan), then warm-up: every lane's device arenas
+    # are allocated on its first batch, so the warm-up runs each lane twice
+    # and writes every y buffer (a first pass over cold lanes ran at up to
+    # 186 us of host work per request instead of ~17)
+    srv.wait(srv.submit(sid, xh_np, y_ring_np[0]))
+    for j in range(4 * 8 * args.e2e_max_batch):
+        srv.submit(sid, xh_np, y_ring_np[j % 8])
     srv.drain()
     srv.reset_stats()
     if dist:
