@@ -657,7 +657,7 @@ def run_ours(args):
             line["details"]["rel_l2_vs_fp64_oracle"] = cpu["checker"]["rel_l2_vs_fp64_oracle"]
             line["e2e"]["rel_l2_vs_fp64_oracle"] = cpu["checker"]["e2e_rel_l2_vs_fp64_oracle"]
         if not args.quick and args.extras and ws == 1:
-            # the other BASELINE configurations, compact, after this
+            # the other benchmark configurations, compact, after this
             # workload's memory is released (results only; the headline
             # above is what the line's value measures)
             del A, B, rp_d, ci_d, v_d, x_d, perm_d, brp, bci, bv, xp, yp
@@ -732,7 +732,7 @@ def small_config(args):
 
 
 def other_configs(args):
-    """The other BASELINE configurations in one run, each compact: the small
+    """The other benchmark configurations in one run, each compact: the small
     R-MAT, the FP16/BF16 precision matrix, the 512-matrix batch and the
     serving pool. A failure is recorded, not raised, so that the headline
     line is always printed."""
