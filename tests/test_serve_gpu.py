@@ -72,9 +72,13 @@ def test_results_match_fp64_and_are_identical_alone_and_mixed(M, O, pool, dtype)
     srv.close()
 
 
-def test_lru_eviction_under_tight_budget(M, O, pool):
-    sizes = [m["reordered"][1].size * 8 + m["perm"].size * 16 for m in pool]
-    srv = M.Server(hbm_budget_bytes=int(sum(sorted(sizes)[-2:]) * 1.3), window_us=100, lanes=2)
+@pytest.mark.parametrize("hub_cache", [False, True])
+def test_lru_eviction_under_tight_budget(M, O, pool, hub_cache):
+    # resident bytes per matrix: CSR + perm and inverse (+ with the hub cache
+    # the remapped colidx and the plan's tables, under 2 MB here)
+    sizes = [m["reordered"][1].size * (12 if hub_cache else 8) + m["perm"].size * 16 + (2 << 20 if hub_cache else 0)
+             for m in pool]
+    srv = M.Server(hbm_budget_bytes=int(sum(sorted(sizes)[-2:]) * 1.3), window_us=100, lanes=2, hub_cache=hub_cache)
     ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
     # one request at a time, cycling over a pool larger than the budget: with
     # LRU every matrix is evicted before it is used again
