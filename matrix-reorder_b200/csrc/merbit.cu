@@ -154,6 +154,10 @@ template <typename V, int SIGMA, int WARPS, int GM>
 __global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOperand<V, SIGMA> m, int tile_num)
 {
     __shared__ __align__(16) float s_buf[WARPS][tile_smem_words<SIGMA>()];
+    // the fix-up grid (launched as a programmatic dependent) may be
+    // scheduled once every CTA of this grid has started; it waits for this
+    // grid's completion before it reads a carry
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int warp = threadIdx.x >> 5;
     const int tile = blockIdx.x * WARPS + warp;
     if (tile >= tile_num) return;
@@ -402,10 +406,14 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
 
 // One thread per tile finishes the short runs that start at its tile; the
 // warp then finishes its lanes' long runs together (whole warps: the grid
-// covers the tiles in blocks of 256).
+// covers the tiles in blocks of 256). Launched as a programmatic dependent
+// of the SpMV grid: its launch and scheduling overlap that grid's last wave,
+// and it waits for that grid's completion (and memory) before any read. In
+// an ordinary launch the wait returns at once.
 __global__ void merbit_fixup_kernel(const uint32_t* __restrict__ tile_y, const float* __restrict__ carry,
                                     int tile_num, int nrow, float* __restrict__ y)
 {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int kind = t < tile_num ? fixup_run_short(tile_y, carry, tile_num, nrow, y, t) : 0;
     unsigned long_runs = __ballot_sync(0xffffffffu, kind == 2);
@@ -446,8 +454,18 @@ static int launch_spmv_t(const MerbitPlan& p, const int* colidx, const void* val
     }
     MR_CUDA_TRY(cudaGetLastError());
     if (p.tile_num > 0) {
-        merbit_fixup_kernel<<<(p.tile_num + 255) / 256, 256, 0, st>>>(p.tile_y, carry, p.tile_num, p.n_rows, y);
-        MR_CUDA_TRY(cudaGetLastError());
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)((p.tile_num + 255) / 256));
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        MR_CUDA_TRY(cudaLaunchKernelEx(&cfg, merbit_fixup_kernel, (const uint32_t*)p.tile_y, (const float*)carry,
+                                       p.tile_num, p.n_rows, y));
     }
     return MR_OK;
 }
