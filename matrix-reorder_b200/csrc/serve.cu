@@ -20,9 +20,9 @@
 //  * Batching: a scheduler thread waits `window_us` after the first pending
 //    request (or until max_batch are pending), takes the pending requests in
 //    arrival order, admits their matrices and launches the batch on a free
-//    lane (a set of buffers and events); up to `lanes` batches are in flight, so requests that
-//    arrive while others are on the GPU form the next batch and overlap on
-//    the device (continuous batching). A batch is: the H2D copies of its x
+//    lane (a set of buffers and events); up to `lanes` batches are in
+//    flight, so requests that arrive while others are on the GPU form the
+//    next batch and overlap on the device (continuous batching). A batch is: the H2D copies of its x
 //    vectors, one batched permutation, the batched MERBIT kernels (one per
 //    (sigma, dtype) group; with `hub_cache`, each matrix's own persistent
 //    plan with the hub cache instead, one launch per item), one batched
