@@ -29,7 +29,7 @@
 //    un-permutation, the D2H copies. The
 //    scheduler issues a batch without holding the server lock, so submits
 //    are never blocked behind the launch.
-//  * Host vectors: x and y of 256 KB and more in page-locked memory
+//  * Host vectors: x and y of 1 MB and more in page-locked memory
 //    (cudaHostAlloc, or cudaHostRegister over the whole vector) are copied
 //    by the copy engines straight from / into the caller's buffer; smaller
 //    ones, and host memory that is not page-locked, go through the lane's
@@ -140,8 +140,11 @@ bool host_pinned(const void* p)
 // for all of them): every DMA has a fixed cost, and with both directions
 // busy, a batch's small copies cut each direction's throughput by about a
 // third (32 copies of log-uniform 16 KB .. 8 MB: 31 GB/s per direction;
-// staging those below 256 KB: 39 GB/s; one copy per direction: 47 GB/s).
-constexpr size_t kStageBelowBytes = 256 << 10;
+// staging those below 256 KB: 36-39 GB/s; below 1 MB: 38-43 GB/s for 0.5-0.8
+// ms of host memcpy per batch; one copy per direction: 47 GB/s). How much a
+// small DMA costs varies between hosts: on a 200-matrix serving pool one
+// box saturated at 15-20K req/s with 256 KB and at 24K with 1 MB.
+constexpr size_t kStageBelowBytes = 1 << 20;
 
 struct Request {
     uint64_t ticket = 0;

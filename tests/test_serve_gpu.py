@@ -175,13 +175,13 @@ def test_loadgen_poisson(M, pool):
 
 
 def _big_pool(M):
-    """Matrices whose vectors straddle the staging threshold (256 KB = 65,536
-    floats): R-MAT scale 12 and 15 (staged) and 17 (copied directly when the
+    """Matrices whose vectors straddle the staging threshold (1 MB = 262,144
+    floats): R-MAT scale 12 and 15 (staged) and 19 (copied directly when the
     vectors are page-locked)."""
     import pyoracle as O
     mats = []
-    for i, sc in enumerate((12, 17, 15)):
-        rp, ci, v = M.gen_rmat(scale=sc, edge_factor=12, seed=30 + i)
+    for i, sc in enumerate((12, 19, 15)):
+        rp, ci, v = M.gen_rmat(scale=sc, edge_factor=8 if sc > 16 else 12, seed=30 + i)
         n2o = M.pgorder(rp, ci, 0, 5)
         perm = np.empty(rp.size - 1, np.int32)
         perm[n2o] = np.arange(rp.size - 1, dtype=np.int32)
