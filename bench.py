@@ -1325,7 +1325,7 @@ def run_batch(args):
     return 0
 
 
-def main() -> int:
+def parser() -> argparse.ArgumentParser:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4000)
@@ -1365,7 +1365,11 @@ def main() -> int:
     ap.add_argument("--sat-requests", type=int, default=20000)
     ap.add_argument("--plain-requests", type=int, default=2000)
     ap.add_argument("--batch-count", type=int, default=512, help="batch: matrices in the graph launch")
-    args = ap.parse_args()
+    return ap
+
+
+def main() -> int:
+    args = parser().parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
