@@ -682,14 +682,21 @@ class Server:
         self._inflight = {}  # ticket -> (x, y): the server reads x / writes y until the request ends
 
     def add_matrix(self, rowptr, colidx, vals, perm_old2new=None) -> int:
+        """vals: numpy float32 / float16, or a host torch bfloat16 tensor."""
         rowptr = np.ascontiguousarray(rowptr, np.int32)
         colidx = np.ascontiguousarray(colidx, np.int32)
-        if vals.dtype == np.float32:
+        if str(getattr(vals, "dtype", "")) == "torch.bfloat16":
+            import torch
+            if vals.is_cuda:
+                raise ValueError("vals must be host memory")
+            vals = vals.contiguous().view(torch.int16).numpy()  # the BF16 bits
+            dt = MR_BF16
+        elif vals.dtype == np.float32:
             dt = MR_F32
         elif vals.dtype == np.float16:
             dt = MR_F16
         else:
-            raise ValueError("vals must be float32 or float16")
+            raise ValueError("vals must be float32, float16 or a bfloat16 tensor")
         vals = np.ascontiguousarray(vals)
         perm = None if perm_old2new is None else np.ascontiguousarray(perm_old2new, np.int32)
         self._keep.append((rowptr, colidx, vals, perm))

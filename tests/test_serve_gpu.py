@@ -222,13 +222,23 @@ def test_staged_and_direct_copies_in_one_batch(M, O, hub_cache):
     srv.close()
 
 
-def test_hub_cache_server_matches_batched_server(M, pool):
+@pytest.mark.parametrize("dtype", [np.float32, np.float16, "bf16"])
+def test_hub_cache_server_matches_batched_server(M, pool, dtype):
     """The same requests through a server of batched plans and one of
-    persistent hub-cache plans: the same SpMV up to summation order."""
+    persistent hub-cache plans, for FP32, FP16 and BF16 values: the same SpMV
+    up to summation order."""
+    import torch
     outs = []
     for hub in (False, True):
         srv = M.Server(window_us=200, lanes=3, hub_cache=hub)
-        ids = [srv.add_matrix(*m["reordered"], m["perm"]) for m in pool]
+        ids = []
+        for m in pool:
+            brp, bci, bv = m["reordered"]
+            if dtype == "bf16":
+                vals = torch.from_numpy(bv).to(torch.bfloat16)
+            else:
+                vals = bv.astype(dtype)
+            ids.append(srv.add_matrix(brp, bci, vals, m["perm"]))
         ys = []
         for j, m in enumerate(pool):
             x = M.uniform(m["perm"].size, seed=300 + j)
