@@ -181,7 +181,15 @@ __global__ void __launch_bounds__(WARPS * 32) merbit_spmv_kernel(const MerbitOpe
 // to finish (atomic ticket after a fence); plans without a table leave
 // every crossing run to the last CTA. Same FP64 run sums, same order, as the
 // two-kernel form: the results are bit-identical.
+//
+// Inside a chunk the warps take the first three quarters of the tiles round
+// robin (warp w: tiles w, w + 32, ...; the 32 warps stay on 32 adjacent
+// tiles) and the rest one at a time from a shared-memory counter, so that
+// warps whose tiles were cheap take more of the tail instead of waiting at the
+// barrier for the slowest (tile costs vary ~30%; a fully counter-driven loop
+// is slower). Which warp runs a tile does not change its result.
 constexpr int kPersistWarps = 32;
+constexpr int kStaticNum = 3, kStaticDen = 4;
 
 __device__ __forceinline__ int open_row(const uint32_t* tile_y, int t) { return tile_open_row(tile_y, t); }
 
@@ -267,7 +275,7 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
                              const int4* __restrict__ brun, int* __restrict__ bflag)
 {
     extern __shared__ __align__(16) float s_dyn[];
-    __shared__ int s_last, s_nlong, s_arrive[2];
+    __shared__ int s_last, s_nlong, s_arrive[2], s_next;
     const int warp = threadIdx.x >> 5;
     const int G = gridDim.x;
     const int chunk = (tile_num + G - 1) / G;
@@ -280,6 +288,10 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
     float* s = s_dyn + warp * tile_smem_words<SIGMA>();
     const TilePolicy pol{l2_evict_last_policy(), l2_evict_first_policy()};
     MerbitOperand<V, SIGMA> m = m_in;
+    // tiles [t0, t0 + nstat) round robin, the rest from the counter s_next
+    const int nstat = (t1 - t0) / kPersistWarps * kStaticNum / kStaticDen * kPersistWarps;
+    if (threadIdx.x == 0) s_next = t0 + nstat;
+    if constexpr (!HUB) __syncthreads();
     if constexpr (HUB) {
         // stage x of the hub columns once per CTA
         float* hub = s_dyn + kPersistWarps * tile_smem_words<SIGMA>();
@@ -304,7 +316,14 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 1)
         m.hub = hub;
         __syncthreads();
     }
-    for (int t = t0 + warp; t < t1; t += kPersistWarps) merbit_tile<V, SIGMA, true, HUB, GM>(m, t, s, pol);
+    for (int t = t0 + warp; t < t0 + nstat; t += kPersistWarps) merbit_tile<V, SIGMA, true, HUB, GM>(m, t, s, pol);
+    for (;;) {
+        int t = 0;
+        if ((threadIdx.x & 31) == 0) t = atomicAdd(&s_next, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= t1) break;
+        merbit_tile<V, SIGMA, true, HUB, GM>(m, t, s, pol);
+    }
     __syncthreads();
     // runs inside the chunk: open rows and carries staged in the (now free)
     // tile staging memory, so a run is walked in shared memory rather than
