@@ -198,26 +198,49 @@ __device__ __forceinline__ void csr_stream_rows(int ra, int rb, const int* __res
     }
 }
 
-// Smallest row i in [0, n] with i + rowptr[i] >= d: the row where the
-// merge path of (rows, nonzeros) crosses diagonal d. Warp-wide 33-ary search.
-__device__ __forceinline__ int csr_merge_row(const int* __restrict__ rowptr, int n, long long d, int lane)
+// For each of two diagonals d: the smallest row i in [0, n] with
+// i + rowptr[i] >= d, the row where the merge path of (rows, nonzeros)
+// crosses d. Warp-wide 33-ary searches (the answer lies in [lo, hi], with
+// g(hi) >= d), the two in lockstep: their probes are issued together, so the
+// warp waits for one chain of dependent loads instead of two.
+__device__ __forceinline__ int2 csr_merge_rows2(const int* __restrict__ rowptr, int n, long long d0, long long d1,
+                                                int lane)
 {
-    int lo = 0, hi = n;  // the answer lies in [lo, hi]; g(hi) >= d
-    while (hi - lo > 32) {
-        const long long span = hi - lo;
-        const int q = lo + (int)(span * (lane + 1) / 33);  // strictly inside (lo, hi)
-        const bool ge = (long long)q + __ldg(rowptr + q) >= d;
-        const unsigned m = __ballot_sync(0xffffffffu, ge);
-        const int f = m ? __ffs(m) - 1 : 32;  // first probe at or past d
-        const int qf = __shfl_sync(0xffffffffu, q, f & 31);
-        const int qp = __shfl_sync(0xffffffffu, q, (f + 31) & 31);
-        if (f < 32) hi = qf;
-        if (f > 0) lo = qp + 1;
+    int lo[2] = {0, 0}, hi[2] = {n, n};
+    const long long d[2] = {d0, d1};
+    while (hi[0] - lo[0] > 32 || hi[1] - lo[1] > 32) {
+        int q[2];
+        bool ge[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const long long span = hi[k] - lo[k];
+            q[k] = lo[k] + (int)(span * (lane + 1) / 33);
+            ge[k] = span > 32 && (long long)q[k] + __ldg(rowptr + q[k]) >= d[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (hi[k] - lo[k] <= 32) continue;  // this search is done (warp-uniform)
+            const unsigned m = __ballot_sync(0xffffffffu, ge[k]);
+            const int f = m ? __ffs(m) - 1 : 32;
+            const int qf = __shfl_sync(0xffffffffu, q[k], f & 31);
+            const int qp = __shfl_sync(0xffffffffu, q[k], (f + 31) & 31);
+            if (f < 32) hi[k] = qf;
+            if (f > 0) lo[k] = qp + 1;
+        }
     }
-    const int q = lo + lane;
-    const bool ge = q <= hi && (long long)q + __ldg(rowptr + q) >= d;
-    const unsigned m = __ballot_sync(0xffffffffu, ge);
-    return m ? lo + __ffs(m) - 1 : hi;
+    int r[2];
+    bool ge[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int q = lo[k] + lane;
+        ge[k] = q <= hi[k] && (long long)q + __ldg(rowptr + q) >= d[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const unsigned m = __ballot_sync(0xffffffffu, ge[k]);
+        r[k] = m ? lo[k] + __ffs(m) - 1 : hi[k];
+    }
+    return make_int2(r[0], r[1]);
 }
 
 // Each warp owns the rows between two merge-path diagonals, an equal share
@@ -234,15 +257,27 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32)
     const int warps = (gridDim.x * blockDim.x) >> 5;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long total = (long long)n + nnz;
-    const int r0 = warp == 0 ? 0 : csr_merge_row(rowptr, n, total * warp / warps, lane);
-    const int r1 = warp == warps - 1 ? n : csr_merge_row(rowptr, n, total * (warp + 1) / warps, lane);
+    const int2 rr = csr_merge_rows2(rowptr, n, total * warp / warps, total * (warp + 1) / warps, lane);
+    const int r0 = warp == 0 ? 0 : rr.x;
+    const int r1 = warp == warps - 1 ? n : rr.y;
+    // row lengths 128 rows at a time, every load of a round in flight
     bool has_long = false;
-    for (int r = r0 + lane; r < r1; r += 32) {
-        const int len = __ldg(rowptr + r + 1) - __ldg(rowptr + r);
-        if (len == 0) y[r] = 0.f;
-        else if (len > kLongRow) {
-            long_rows[atomicAdd(n_long, 1)] = r;
-            has_long = true;
+    for (int base = r0; base < r1; base += 4 * 32) {
+        int len[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = base + lane + 32 * j;
+            len[j] = r < r1 ? __ldg(rowptr + r + 1) - __ldg(rowptr + r) : 1;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = base + lane + 32 * j;
+            if (r >= r1) continue;
+            if (len[j] == 0) y[r] = 0.f;
+            else if (len[j] > kLongRow) {
+                long_rows[atomicAdd(n_long, 1)] = r;
+                has_long = true;
+            }
         }
     }
     if (!__any_sync(0xffffffffu, has_long)) {
