@@ -160,10 +160,10 @@ int mr_spmv_merbit(const mr_merbit_plan* plan, const mr_csr_view* A, const float
  * and y as for mr_spmv_merbit. Each call checks the matrix as plan creation
  * does and waits for that check on `stream` (a malformed rowptr or column
  * index returns MR_ERR_INVALID_ARG before any gather), then rebuilds the
- * plan into the array and gives bitwise the result of a planned call. The
- * wait for the check makes a call impossible to capture into a CUDA graph.
- * The first call on a device looks up the array's device address and keeps
- * it: make no call after cudaDeviceReset. All calls share the array, so
+ * plan into the array and gives bitwise the result of a planned call.
+ * The first call on a device does a set-up: it looks up the array's device
+ * address and keeps it, so make that first call before any stream capture
+ * and make no call after cudaDeviceReset. All calls share the array, so
  * calls that overlap on the GPU race: order them on one stream. */
 int mr_spmv_merbit_noalloc(const mr_csr_view* A, const float* x_dev, float* y_dev, void* stream);
 

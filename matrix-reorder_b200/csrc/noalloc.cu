@@ -22,12 +22,12 @@
 //  * it then rebuilds the plan into the array (one extra kernel) and runs
 //    the same persistent MERBIT kernel as mr_spmv_merbit, so results are
 //    bitwise those of a planned call;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current) and keeps it for the
-//    process. The kept address dies with the device's context: after
+//  * the first call on a device does a set-up: it looks up the array's
+//    device address (cudaGetSymbolAddress, with that device current) and
+//    keeps it for the process, so that first call should come before any
+//    stream capture. The kept address dies with the device's context: after
 //    cudaDeviceReset the entry point must not be called again in that
-//    process. (The wait for the matrix check makes every call
-//    synchronise its stream, so no call can be captured into a graph);
+//    process;
 //  * all calls share the array and it keeps the last call's contents, so
 //    calls whose work overlaps on the GPU (different streams, or threads
 //    without ordering) race: serialise them on one stream. Every call
